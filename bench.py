@@ -1,0 +1,312 @@
+"""Throughput of the matrix-free Lindblad path on one or more B200s.
+
+Workload: the 12-qubit open transverse-field Ising chain (Hilbert D = 4096,
+rho = 16.8M complex128 = 268 MB, 35 terms: 11 ZZ + 12 X Hamiltonian terms,
+12 decay + 12 dephasing Lindblad terms; J ~ U[0.5,1.5], h ~ N(0, 0.2^2)
+from a seeded generator).  One bench step is one integration segment of 10
+fixed RK4 steps (dt = 0.01), i.e. 40 fused L.rho stage launches.
+
+metric: L.rho GB/s = applications x 32*D^2 algorithmic bytes (read rho,
+write L rho, 16 B each per element) / time.  `value` has rho resident in
+HBM; `e2e` goes through the C-ABI call quac_time_step_host with the state
+in pinned host memory (H2D + segment + D2H every step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 every rank integrates its own replica (independent systems, no
+collective on the data path); the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "L·ρ GB/s; ensemble & steady-state solves/s vs plain FP64 GPU at ≤1e-8 error"
+NQ = 12
+DT = 0.01
+RK_STEPS = 10
+STAGES = 4 * RK_STEPS
+
+
+def tfim_terms(S, n=NQ, seed=3):
+    import helpers as H
+    return H.tfim(S, n, seed=seed)
+
+
+def workload_config(n_gpus):
+    return {"workload": f"tfim{NQ}_rk4_segment", "D": 2 ** NQ, "rho_bytes": 16 * 4 ** NQ,
+            "rk": "rk4", "rk_steps_per_segment": RK_STEPS, "dt": DT,
+            "lrho_per_step": STAGES, "terms": 47, "parallelism": f"replicas{n_gpus}",
+            "l2": "inputs larger than L2 (268 MB state vs 126 MB L2)"}
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True,
+                                         text=True, timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 3 + k and "Active" in s[3 + k] and "Not" not in s[3 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the L.rho stage kernel from the committed ncu
+    summary (profiles/lrho_tfim12.json), or None."""
+    p = os.path.join(ROOT, "profiles", "lrho_tfim12.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch_full_size")
+    return None
+
+
+def cpu_baseline(seconds=12.0, rows_frac=64):
+    """The oracle's restatement of the reference algorithm (assembled CSR from
+    the kron.c maps, one CSR SpMV per RK stage) on a row block of the same
+    Liouvillian: 1/rows_frac of the rows, timed for about `seconds`."""
+    from oracle import oracle as O
+    S = O.OSys()
+    tfim_terms(S)
+    D = S.D
+    nrows = D * D // rows_frac
+    h = S.csr_handle(rows=(0, nrows))
+    x = np.random.default_rng(0).normal(size=D * D) + 0j
+    y = np.zeros(nrows, dtype=np.complex128)
+    L = O.lib()
+    import ctypes
+    xp, yp = x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p)
+    L.orc_spmv(h, xp, yp)
+    n = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        L.orc_spmv(h, xp, yp)
+        n += 1
+    dt = time.perf_counter() - t0
+    O.free_csr(h)
+    gbs = n * nrows * 32 / dt / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"CSR SpMV over rows [0, D^2/{rows_frac}) of the D=4096 Liouvillian "
+                      f"({nrows} rows), {n} applications in {dt:.1f} s, OpenMP"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    # each step: one RK4 segment's worth (40 applications) of CSR SpMV on the sample rows
+    from oracle import oracle as O
+    import ctypes
+    S = O.OSys()
+    tfim_terms(S)
+    D = S.D
+    frac = 64
+    nrows = D * D // frac
+    h = S.csr_handle(rows=(0, nrows))
+    x = np.random.default_rng(0).normal(size=D * D) + 0j
+    y = np.zeros(nrows, dtype=np.complex128)
+    L = O.lib()
+    xp, yp = x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p)
+    for _ in range(args.warmup):
+        L.orc_spmv(h, xp, yp)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for _ in range(STAGES):
+            L.orc_spmv(h, xp, yp)
+    dt = time.perf_counter() - t0
+    O.free_csr(h)
+    gbs = args.steps * STAGES * nrows * 32 / dt / 1e9
+    sample = (f"each step = {STAGES} CSR SpMV over rows [0, D^2/{frac}) ({nrows} rows) of the "
+              f"assembled D=4096 Liouvillian")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic", "config": workload_config(args.gpus),
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference PETSc build unavailable (PETSc/SLEPc absent); oracle port of the "
+                "reference algorithm timed instead"}))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import quac_b200 as q
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    q.lib()
+    q.QuaC_initialize()
+    import helpers as H
+    S = H.ProductSystem(q)
+    tfim_terms(S)
+    qs = S.qs
+    q.construct_matrix(qs)
+    D = S.D
+    n = D * D
+    rho = q.create_dm_sys(qs)
+    rng = np.random.default_rng(1234 + rank)
+    X = (rng.standard_normal((D, D)) + 1j * rng.standard_normal((D, D))).astype(np.complex128)
+    X = (X + X.conj().T) / 2.0
+    x0 = np.ascontiguousarray(X.reshape(-1, order="F"))
+    rho.from_numpy(x0)
+    stream = torch.cuda.Stream(device=dev)
+    q.set_stream(qs, stream.cuda_stream)
+    q.set_ts_options(rk_type="4", adapt_type="none")
+
+    def segment(t):
+        q.time_step_sys(qs, rho, t, t + RK_STEPS * DT, DT, 10 ** 9)
+
+    t = 0.0
+    for _ in range(args.warmup):
+        segment(t)
+        t += RK_STEPS * DT
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    launches0 = q.kernel_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        segment(t)
+        t += RK_STEPS * DT
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = q.kernel_launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    # e2e through the C ABI with host (pinned) buffers
+    host = torch.from_numpy(x0.copy()).pin_memory()
+    hp = host.numpy()
+    q.set_stream(qs, None)
+    q.time_step_host(qs, hp, 0.0, RK_STEPS * DT, DT, 10 ** 9)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        q.time_step_host(qs, hp, 0.0, RK_STEPS * DT, DT, 10 ** 9)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    ms_t = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(ms_t[0]), float(ms_t[1])
+    alg_bytes = 32.0 * n
+    total_apps = args.steps * STAGES * world
+    value = total_apps * alg_bytes / (ms / 1e3) / 1e9
+    e2e = total_apps * alg_bytes / (e2e_ms / 1e3) / 1e9
+    per_launch_ms = ms / (args.steps * STAGES)
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profiled_traffic()
+    out = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": workload_config(world),
+        "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": 16 * n,
+                "d2h_bytes_per_step": 16 * n},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                     "kernel": "k_lrho (fused RK4 stage)"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline()
+    q.set_ts_options(rk_type="3bs", adapt_type="basic")
+    rho.destroy()
+    qs.destroy()
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,281 @@
+/*
+ * quac_b200.h -- C ABI of the B200 Lindblad engine.
+ *
+ * The entry points keep the names, argument order and meaning of QuaC's C
+ * API so that a QuaC program recompiles against this header (through the
+ * drop-in headers in include/quac/) and links libquac_b200.so instead of
+ * QuaC + PETSc.  Each declaration cites the reference interface it
+ * replaces (path within the QuaC project : line).
+ *
+ * Storage: every qvec lives in GPU memory (complex128).  A density matrix
+ * is column stacked, vec(rho)[D*col + row] = rho[row][col]
+ * (qvec_utilities.c:322-337); subsystem 0 is the most significant Hilbert
+ * digit (kron.c:308).
+ *
+ * Errors: the reference prints and calls exit() on misuse; these entry
+ * points print the same kind of message and exit as well, unless
+ * quac_set_error_mode(QUAC_ERRORS_RETURN) was called, in which case they
+ * record the message (quac_last_error()) and return.  The *_ex variants
+ * always return a status (0 = success).
+ *
+ * PETSc types are replaced by plain C types: PetscScalar = complex double,
+ * PetscInt = int64_t, PetscReal = double, PetscErrorCode = int, and Vec/TS
+ * are opaque handles owned by this library.
+ */
+#ifndef QUAC_B200_H_
+#define QUAC_B200_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+#include <complex>
+typedef std::complex<double> PetscScalar;
+#define PETSC_i (PetscScalar(0.0, 1.0))
+#define PetscRealPart(x) (std::real(x))
+#define PetscImaginaryPart(x) (std::imag(x))
+extern "C" {
+#else
+#include <complex.h>
+typedef double _Complex PetscScalar;
+#define PETSC_i (_Complex_I)
+#define PetscRealPart(x) (creal(x))
+#define PetscImaginaryPart(x) (cimag(x))
+#endif
+
+typedef int64_t PetscInt;
+typedef double PetscReal;
+typedef int PetscErrorCode;
+typedef int PetscBool;
+#define PETSC_TRUE 1
+#define PETSC_FALSE 0
+#define PETSC_COMM_WORLD 0
+#define PetscFunctionReturn(x) return (x)
+
+typedef struct _p_Vec *Vec;          /* device vector handle */
+typedef struct _p_TS *TS;            /* time-stepper handle passed to monitors */
+typedef struct _p_Mat *Mat;          /* assembled-operator handle (export only) */
+
+/* operator types: operators_p.h:6-16 */
+typedef enum {
+  RAISE = -1, NUMBER = 0, LOWER = 1, VEC = 2, SIGMA_X = 3, SIGMA_Y = 4, SIGMA_Z = 5,
+  IDENTITY = 6, OTHER = 7
+} op_type;
+
+/* qvec types: qsystem_p.h:22-26 */
+typedef enum { DENSITY_MATRIX = -1, WAVEFUNCTION = 1, WF_ENSEMBLE = 2 } qvec_type;
+
+/* gate types: quantum_gates.h:11-33 */
+typedef enum {
+  NULL_GATE = -1000, SQiSWP = -8, CZ_ARP = -7, CUSTOM2QGATE = -6, CZX = -5, CmZ = -4, CZ = -3,
+  CXZ = -2, CNOT = -1, HADAMARD = 1, SIGMAX = 2, SIGMAY = 3, SIGMAZ = 4, EYE = 5, RX = 6,
+  RY = 7, RZ = 8, U1 = 9, U2 = 10, U3 = 11, CUSTOM1QGATE = 12
+} gate_type;
+
+/* operator: operators.h:8-33.  Fields a QuaC program reads (dag, n, eye,
+ * sig_x/y/z, other, my_levels, n_before, my_op_type, position) keep their
+ * names and meaning. */
+struct operator_s;
+typedef struct operator_s {
+  double initial_pop;
+  PetscInt initial_exc;
+  PetscInt n_before;
+  PetscInt my_levels;
+  op_type my_op_type;
+  PetscInt pos_in_sys_hspace;
+  struct operator_s *dag, *n, *sig_x, *sig_y, *sig_z, *eye, *other;
+  PetscInt position;
+  struct operator_s **vec_op_list;
+  PetscScalar evals[2];
+  PetscScalar evecs[2][2];
+} *op_handle;
+#ifndef __cplusplus
+typedef op_handle operator;
+#endif
+typedef op_handle *vec_op;
+
+struct quantum_gate_struct;
+typedef void (*custom_gate_func_type)(PetscScalar *, PetscInt, PetscInt, void *);
+
+/* quantum_gates.h:38-48 */
+struct quantum_gate_struct {
+  PetscReal time, run_time;
+  gate_type my_gate_type;
+  PetscInt *qubit_numbers, num_qubits;
+  custom_gate_func_type custom_func;
+  PetscReal theta, phi, lambda;
+  void *gate_ctx;
+};
+
+/* quantum_gates.h:51-55 */
+struct gate_layer_struct {
+  PetscReal time;
+  PetscInt num_gates;
+  struct quantum_gate_struct *gate_list;
+};
+
+/* qsystem_p.h:46-48: user data for CUSTOM1QGATE / CUSTOM2QGATE */
+typedef struct { PetscScalar gate_data[4][4]; } custom_gate_data;
+
+/* circuit: qsystem_p.h:50-55 (a value struct) */
+typedef struct circuit {
+  PetscInt num_gates, gate_list_size, current_gate, num_layers, current_layer;
+  PetscReal start_time;
+  struct quantum_gate_struct *gate_list;
+  struct gate_layer_struct *layer_list;
+} circuit;
+
+/* qvec: qsystem_p.h:60-66 */
+typedef struct qvec_s {
+  qvec_type my_type;
+  PetscBool ens_spawned;
+  PetscInt n, Istart, Iend, total_levels, *hspace_dims, ndims_hspace, n_ops, n_ensemble, ens_i;
+  Vec data;
+  Vec *ens_datas;
+} *qvec;
+
+typedef PetscErrorCode (*quac_ts_monitor)(TS, PetscInt, PetscReal, Vec, void *);
+
+struct qsystem_impl;
+/* qsystem: qsystem_p.h:69-116 (public fields kept; engine state is opaque) */
+typedef struct qsystem_s {
+  PetscInt num_time_indep, num_time_dep;
+  PetscInt hspace_frozen;
+  PetscBool dm_equations, mcwf_solver, time_step_called;
+  PetscInt mat_allocated;
+  PetscInt num_subsystems;
+  op_handle *subsystem_list;
+  PetscInt total_levels, dim;
+  qvec solution_qvec;
+  PetscInt np, nid;
+  PetscReal current_time;
+  quac_ts_monitor ts_monitor;
+  void *ts_ctx;
+  PetscInt num_circuits, circuit_list_size, current_circuit;
+  circuit *circuit_list;
+  struct qsystem_impl *impl;
+} *qsystem;
+
+/* ------------------------------------------------------------ runtime */
+void QuaC_initialize(int argc, char **args);           /* quac.c:25-58 */
+void QuaC_finalize(void);                               /* quac.c:89-111 */
+void QuaC_clear(void);                                  /* quac.c:60-87 */
+int PetscPrintf(int comm, const char *fmt, ...);        /* PETSc printing, rank 0 only */
+
+/* ----------------------------------------------------- system building */
+void initialize_system(qsystem *qsys);                  /* qsystem.c:16-70 */
+void destroy_system(qsystem *qsys);                     /* qsystem.c:72-91 */
+void create_op_sys(qsystem qsys, PetscInt levels, op_handle *op);      /* qsystem.c:153-230 */
+void destroy_op_sys(op_handle *op);                     /* qsystem.c:349-361 */
+void create_vec_op_sys(qsystem qsys, PetscInt levels, vec_op *vop);    /* qsystem.c:276-329 */
+void destroy_vec_op_sys(vec_op *vop);                   /* qsystem.c:331-340 */
+void set_init_excited_op(op_handle op, PetscInt initial_exc);           /* qsystem.c:1339-1349 */
+void add_ham_term(qsystem qsys, PetscScalar a, PetscInt num_ops, ...); /* qsystem.c:407-434 */
+void add_lin_term(qsystem qsys, PetscScalar a, PetscInt num_ops, ...); /* qsystem.c:436-462 */
+void add_lin_term_list(qsystem qsys, PetscScalar a, PetscInt num_ops, op_handle *ops); /* qsystem.c:464-489 */
+void add_ham_term_list(qsystem qsys, PetscScalar a, PetscInt num_ops, op_handle *ops); /* list form of qsystem.c:407-434 */
+void clear_mat_terms_sys(qsystem qsys);                 /* qsystem.c:557-591 */
+void construct_matrix(qsystem qsys);                    /* qsystem.c:593-676 */
+void use_mcwf_solver(qsystem qsys, PetscInt num_tot_trajs, PetscInt seed); /* qsystem.c:358-403 */
+
+/* ---------------------------------------------------------- time steps */
+/* qsystem.c:895-1098.  Default scheme: Bogacki-Shampine 3(2), adaptive,
+ * atol = rtol = 5e-7, step limits [0.01, 1], final step matched to tmax;
+ * QuaC_initialize's -ts_rk_type / -ts_adapt_type / -ts_rtol / -ts_atol /
+ * -ts_max_steps options override these as TSSetFromOptions does. */
+void time_step_sys(qsystem qsys, qvec x, PetscReal t0, PetscReal tmax, PetscReal dt,
+                   PetscInt steps_max);
+void set_ts_monitor_sys(qsystem qsys, quac_ts_monitor monitor, void *ctx); /* qsystem.c:875-879 */
+
+/* --------------------------------------------------------------- qvecs */
+void create_qvec_sys(qsystem qsys, qvec *q);            /* qvec_utilities.c:633-648 */
+void create_dm_sys(qsystem qsys, qvec *q);              /* qvec_utilities.c:650-703 */
+void create_wf_sys(qsystem qsys, qvec *q);              /* qvec_utilities.c:705-763 */
+void create_arb_qvec(qvec *q, PetscInt nstates, qvec_type type);      /* qvec_utilities.c:471-521 */
+void destroy_qvec(qvec *q);                             /* qvec_utilities.c:1076-1091 */
+void add_to_qvec(qvec q, PetscScalar alpha, ...);       /* qvec_utilities.c:919-969 */
+void add_to_qvec_loc(qvec q, PetscScalar alpha, PetscInt loc);        /* qvec_utilities.c:879-897 */
+void assemble_qvec(qvec q);                             /* qvec_utilities.c:1047-1066 */
+void set_qvec_from_init_excited_op(qsystem qsys, qvec q);             /* qvec_utilities.c:2540-2566 */
+void get_dm_element_qvec(qvec q, PetscInt row, PetscInt col, PetscScalar *val); /* qvec_utilities.c:322-337 */
+void get_wf_element_qvec(qvec q, PetscInt loc, PetscScalar *val);     /* qvec_utilities.c:409-414 */
+void get_trace_qvec(qvec q, PetscScalar *val);          /* qvec_utilities.c:378-392 */
+void get_expectation_value_qvec(qvec q, PetscScalar *val, PetscInt num_ops, ...); /* qvec_utilities.c:1133-1150 */
+void get_expectation_value_qvec_list(qvec q, PetscScalar *val, PetscInt num_ops, op_handle *ops); /* qvec_utilities.c:1176-1195 */
+void get_fidelity_qvec(qvec q1, qvec q2, PetscReal *fidelity, PetscReal *var); /* qvec_utilities.c:2159-2245 (dm-wf, wf-wf) */
+void get_bitstring_probs(qvec q, PetscInt *nloc, PetscReal **probs, PetscReal **vars); /* qvec_utilities.c:1682-1718 */
+void copy_qvec(qvec src, qvec dst);                     /* qvec_utilities.c:33-55 */
+void print_qvec(qvec q);                                /* qvec_utilities.c:277-289 */
+void read_qvec_dm_binary(qvec *q, const char filename[]);  /* qvec_utilities.c:129-167 */
+void read_qvec_wf_binary(qvec *q, const char filename[]);  /* qvec_utilities.c:97-127 */
+void print_qvec_file(qvec q, char filename[]);           /* PETSc-binary Vec writer (qvec_utilities.c:203-212 writes text; this writes the binary format read above) */
+
+/* ------------------------------------------------------------ circuits */
+void create_circuit(circuit *circ, PetscInt num_gates); /* quantum_gates.c:610-632 */
+void destroy_circuit(circuit *circ);                    /* quantum_gates.c:634-641 */
+void add_gate_to_circuit_sys(circuit *circ, PetscReal time, gate_type g, ...); /* quantum_circuits.c:172-255 */
+void schedule_circuit_layers(qsystem qsys, circuit *circ);            /* quantum_circuits.c:316-404 */
+void apply_circuit_to_sys(qsystem qsys, circuit *circ, PetscReal time); /* quantum_circuits.c:407-431 */
+void apply_circuit_to_qvec(qsystem qsys, circuit circ, qvec q);       /* quantum_circuits.c:143-159 */
+void apply_gate2(qvec q, gate_type g, ...);             /* quantum_circuits.c:776-847 */
+
+/* ------------------------------------------------- legacy global API */
+void create_op(int levels, op_handle *op);              /* operators.c:59-200 */
+void create_vec(int levels, vec_op *vop);               /* operators.c:210-242 */
+void destroy_op(op_handle *op);                         /* quac.c:113-126 */
+void destroy_vec(vec_op *vop);                          /* quac.c:128-141 */
+void add_to_ham(PetscScalar a, op_handle op);           /* operators.c:290-337 */
+void add_to_ham_mult2(PetscScalar a, op_handle op1, op_handle op2);   /* operators.c:405-488 */
+void add_to_ham_mult3(PetscScalar a, op_handle op1, op_handle op2, op_handle op3); /* operators.c:601-663 */
+void add_lin(PetscScalar a, op_handle op);              /* operators.c:679-719 */
+void add_lin_mult2(PetscScalar a, op_handle op1, op_handle op2);      /* operators.c:743-821 */
+void steady_state(Vec x);                               /* solver.c:33-221 */
+void set_ts_monitor(quac_ts_monitor monitor);           /* solver.c:526-532 */
+
+/* --------------------------------------------- PETSc Vec/TS stand-ins */
+PetscErrorCode VecGetArray(Vec v, PetscScalar **a);     /* maps the data to host memory */
+PetscErrorCode VecRestoreArray(Vec v, PetscScalar **a); /* writes host changes back */
+PetscErrorCode VecGetSize(Vec v, PetscInt *n);
+PetscErrorCode VecDuplicate(Vec v, Vec *out);
+PetscErrorCode VecCopy(Vec src, Vec dst);
+PetscErrorCode VecDestroy(Vec *v);
+PetscErrorCode VecCreateSeq(int comm, PetscInt n, Vec *v);
+PetscErrorCode TSGetTime(TS ts, PetscReal *t);
+PetscErrorCode TSGetTimeStep(TS ts, PetscReal *dt);
+
+/* ------------------------------- entry points with no QuaC counterpart */
+/* Steady state of a qsystem (the reference only offers the legacy global
+ * form, solver.c:33-221): solves (L + e0 vec(I)^T) x = e0 by restarted
+ * GMRES on the GPU; returns the iterations used, or -1 on failure. */
+PetscInt steady_state_sys(qsystem qsys, qvec x);
+/* One application y = L x of the constructed Liouvillian on device
+ * buffers of qsys->dim complex128 values (the TSComputeRHSFunctionLinear
+ * action, qsystem.c:937).  Returns 0 on success. */
+int quac_lrho_apply_device(qsystem qsys, const void *x_dev, void *y_dev);
+/* Same on host buffers: copies x in, applies L, copies y out. */
+int quac_lrho_apply_host(qsystem qsys, const PetscScalar *x_host, PetscScalar *y_host);
+/* Time-steps host data in place: one call = H2D + integration + D2H. */
+int quac_time_step_host(qsystem qsys, PetscScalar *x_host, PetscReal t0, PetscReal tmax,
+                        PetscReal dt, PetscInt steps_max);
+
+#define QUAC_ERRORS_EXIT 0
+#define QUAC_ERRORS_RETURN 1
+void quac_set_error_mode(int mode);
+const char *quac_last_error(void);
+void quac_clear_error(void);
+/* Integrator selection without argv: scheme "3bs" | "4" | "5dp",
+ * adapt "basic" | "none"; non-positive tolerances keep the current ones. */
+int quac_set_ts_options(const char *rk_type, const char *adapt_type, double rtol, double atol,
+                        PetscInt max_steps);
+/* Device pointer of a qvec (complex128, qvec->n values). */
+void *quac_qvec_device_ptr(qvec q);
+/* Launch this system's kernels on a caller-owned CUDA stream (NULL: the
+ * library's own stream). */
+void quac_set_stream(qsystem qsys, void *cuda_stream);
+/* Number of kernels this library has launched (diagnostics). */
+int64_t quac_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QUAC_B200_H_ */

@@ -251,33 +251,58 @@ csr *orc_build(int nsub, const i64 *levels, int nterms, const int *kind, const d
   i64 dim = (mode == 0) ? D * D : D;
   if (row1 < 0 || row1 > dim) row1 = dim;
   coo m = {0};
+  /* columns whose rows intersect [row0,row1) (density-matrix mode) */
+  i64 cfirst = row0 / D, clast = (row1 + D - 1) / D;
   for (int t = 0; t < nterms; t++) {
     oterm *tm = &T[t];
     if (mode == 0) {
+      /* the (G^T x I) parts only move the column digit: evaluate them once
+       * per column (value independent of the row digit) and emit the rows
+       * that land in the block */
+      i64 *cmap = malloc(D * sizeof(i64));
+      cplx *cval = malloc(D * sizeof(cplx));
+      for (i64 c = 0; c < D; c++) {
+        i64 j = c * D; cplx v;
+        val_j_ops(&s, &j, &v, tm->nops, tm->ops, T_GI);
+        cmap[c] = (j == -1) ? -1 : j / D;
+        cval[c] = v;
+      }
       if (tm->kind == 1) {
-        for (i64 i = 0; i < dim; i++) {
-          i64 jig = i, jgi = i; cplx vig, vgi;
+        for (i64 i = row0; i < row1; i++) {
+          i64 jig = i; cplx vig;
           val_j_ops(&s, &jig, &vig, tm->nops, tm->ops, T_IG);
-          val_j_ops(&s, &jgi, &vgi, tm->nops, tm->ops, T_GI);
-          if (jig != -1 && i >= row0 && i < row1) coo_push(&m, i, jig, -tm->a * I * vig);
-          if (jgi != -1 && jgi >= row0 && jgi < row1) {
-            cplx aa = conj_compat ? conj(tm->a) : tm->a;
-            coo_push(&m, jgi, i, aa * I * conj(vgi));
+          if (jig != -1) coo_push(&m, i, jig, -tm->a * I * vig);
+        }
+        cplx aa = conj_compat ? conj(tm->a) : tm->a;
+        for (i64 c = 0; c < D; c++) {
+          if (cmap[c] < 0 || cmap[c] < cfirst || cmap[c] >= clast) continue;
+          for (i64 r = 0; r < D; r++) {
+            i64 tgt = cmap[c] * D + r;
+            if (tgt >= row0 && tgt < row1) coo_push(&m, tgt, c * D + r, aa * I * conj(cval[c]));
           }
         }
       } else {
-        for (i64 i = 0; i < dim; i++) {
-          i64 jig = i, jgi = i, jgg = i; cplx vig, vgi, vgg;
+        for (i64 i = cfirst * D; i < clast * D && i < dim; i++) {
+          i64 jig = i; cplx vig;
           val_j_ops(&s, &jig, &vig, tm->nops, tm->ops, T_IG);
-          val_j_ops(&s, &jgi, &vgi, tm->nops, tm->ops, T_GI);
-          val_j_ops(&s, &jgg, &vgg, tm->nops, tm->ops, T_GG);
           if (jig != -1 && jig >= row0 && jig < row1)
             coo_push(&m, jig, jig, -0.5 * tm->a * conj(vig) * vig);
-          if (jgi != -1 && jgi >= row0 && jgi < row1)
-            coo_push(&m, jgi, jgi, -0.5 * tm->a * conj(conj(vgi) * vgi));
-          if (jgg != -1 && i >= row0 && i < row1) coo_push(&m, i, jgg, tm->a * vgg);
+        }
+        for (i64 c = 0; c < D; c++) {
+          if (cmap[c] < 0 || cmap[c] < cfirst || cmap[c] >= clast) continue;
+          for (i64 r = 0; r < D; r++) {
+            i64 tgt = cmap[c] * D + r;
+            if (tgt >= row0 && tgt < row1)
+              coo_push(&m, tgt, tgt, -0.5 * tm->a * conj(conj(cval[c]) * cval[c]));
+          }
+        }
+        for (i64 i = row0; i < row1; i++) {
+          i64 jgg = i; cplx vgg;
+          val_j_ops(&s, &jgg, &vgg, tm->nops, tm->ops, T_GG);
+          if (jgg != -1) coo_push(&m, i, jgg, tm->a * vgg);
         }
       }
+      free(cmap); free(cval);
     } else {
       if (tm->kind == 1) {
         for (i64 i = row0; i < row1; i++) {
@@ -704,9 +729,12 @@ csr *orc_add_trace_row(const csr *A, i64 D) {
   return B;
 }
 
-/* GMRES(m) with left ILU(0) preconditioning, classical Gram-Schmidt, on the
- * stabilised operator, b = x0 = e0 (solver.c:143-198).  Converges when the
- * preconditioned residual drops by rtol.  Returns iterations used. */
+/* GMRES(m) with right ILU(0) preconditioning (A M^-1 y = b, x = M^-1 y),
+ * classical Gram-Schmidt, on the stabilised operator with b = x0 = e0
+ * (solver.c:143-198).  Right preconditioning keeps the Arnoldi residual
+ * equal to the true residual ||b - A x||, which is the quantity the
+ * steady-state comparison is judged on (PETSc's default is left
+ * preconditioning; the fixed point is the same).  Returns iterations. */
 i64 orc_gmres_ilu(const csr *B, double *xd, double rtol, int restart, i64 maxit, int use_ilu) {
   i64 n = B->nrows;
   cplx *x = (cplx *)xd;
@@ -717,32 +745,30 @@ i64 orc_gmres_ilu(const csr *B, double *xd, double rtol, int restart, i64 maxit,
   cplx *cs = malloc(m * sizeof(cplx)), *sn = malloc(m * sizeof(cplx)), *g = malloc((m + 1) * sizeof(cplx));
   cplx *w = malloc(n * sizeof(cplx)), *t = malloc(n * sizeof(cplx)), *b = calloc(n, sizeof(cplx));
   b[0] = 1.0;
-  /* preconditioned rhs norm */
-  if (F) ilu0_solve(F, b, t); else memcpy(t, b, n * sizeof(cplx));
-  double bnorm = nrm2(n, t);
+  double bnorm = 1.0;
   i64 it = 0;
   while (it < maxit) {
     orc_spmv(B, (double *)x, (double *)w);
     for (i64 i = 0; i < n; i++) w[i] = b[i] - w[i];
-    if (F) ilu0_solve(F, w, t); else memcpy(t, w, n * sizeof(cplx));
-    double beta = nrm2(n, t);
+    double beta = nrm2(n, w);
     if (beta <= rtol * bnorm) break;
-    for (i64 i = 0; i < n; i++) V[i] = t[i] / beta;
+    for (i64 i = 0; i < n; i++) V[i] = w[i] / beta;
     for (int k = 0; k <= m; k++) g[k] = 0;
     g[0] = beta;
     int j;
     for (j = 0; j < m && it < maxit; j++, it++) {
-      orc_spmv(B, (double *)(V + (size_t)j * n), (double *)w);
-      if (F) ilu0_solve(F, w, t); else memcpy(t, w, n * sizeof(cplx));
+      const cplx *vj = V + (size_t)j * n;
+      if (F) ilu0_solve(F, vj, t); else memcpy(t, vj, n * sizeof(cplx));
+      orc_spmv(B, (double *)t, (double *)w);
       for (int k = 0; k <= j; k++) {
         cplx h = 0; const cplx *vk = V + (size_t)k * n;
-        for (i64 i = 0; i < n; i++) h += conj(vk[i]) * t[i];
+        for (i64 i = 0; i < n; i++) h += conj(vk[i]) * w[i];
         H[k * m + j] = h;
-        for (i64 i = 0; i < n; i++) t[i] -= h * vk[i];
+        for (i64 i = 0; i < n; i++) w[i] -= h * vk[i];
       }
-      double hn = nrm2(n, t);
+      double hn = nrm2(n, w);
       H[(j + 1) * m + j] = hn;
-      if (hn > 0) for (i64 i = 0; i < n; i++) V[(size_t)(j + 1) * n + i] = t[i] / hn;
+      if (hn > 0) for (i64 i = 0; i < n; i++) V[(size_t)(j + 1) * n + i] = w[i] / hn;
       for (int k = 0; k < j; k++) {
         cplx a = H[k * m + j], bb = H[(k + 1) * m + j];
         H[k * m + j] = conj(cs[k]) * a + conj(sn[k]) * bb;
@@ -757,19 +783,21 @@ i64 orc_gmres_ilu(const csr *B, double *xd, double rtol, int restart, i64 maxit,
       g[j] = conj(cs[j]) * g[j];
       if (cabs(g[j + 1]) <= rtol * bnorm) { j++; it++; break; }
     }
-    /* back substitution and update */
-    cplx *yv = calloc(j, sizeof(cplx));
+    cplx *yv = calloc(j > 0 ? j : 1, sizeof(cplx));
     for (int k = j - 1; k >= 0; k--) {
       cplx s = g[k];
       for (int q = k + 1; q < j; q++) s -= H[k * m + q] * yv[q];
       yv[k] = s / H[k * m + k];
     }
+    /* x += M^-1 (V y) */
+    for (i64 i = 0; i < n; i++) w[i] = 0;
     for (int k = 0; k < j; k++) {
       const cplx *vk = V + (size_t)k * n;
-      for (i64 i = 0; i < n; i++) x[i] += yv[k] * vk[i];
+      for (i64 i = 0; i < n; i++) w[i] += yv[k] * vk[i];
     }
+    if (F) ilu0_solve(F, w, t); else memcpy(t, w, n * sizeof(cplx));
+    for (i64 i = 0; i < n; i++) x[i] += t[i];
     free(yv);
-    if (j > 0 && cabs(g[j]) <= rtol * bnorm) break;
   }
   free(V); free(H); free(cs); free(sn); free(g); free(w); free(t); free(b);
   if (F) { free(F->lu); free(F->diag); free(F); }

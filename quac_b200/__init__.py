@@ -1,0 +1,626 @@
+"""Python mirror of QuaC's C API over libquac_b200.so (ctypes).
+
+The names follow the reference (QuaC, src/qsystem.h, src/qvec_utilities.h,
+src/quantum_circuits.h, src/solver.h) so a QuaC program reads the same
+here::
+
+    import quac_b200 as q
+    q.QuaC_initialize()
+    qs = q.initialize_system()
+    qb = q.create_op_sys(qs, 2)
+    cav = q.create_op_sys(qs, 10)
+    q.add_ham_term(qs, 0.1, cav.dag, qb)
+    q.add_lin_term(qs, 1e-2, cav)
+    q.construct_matrix(qs)
+    rho = q.create_qvec_sys(qs)
+    q.add_to_qvec(rho, 1.0, 10, 10)
+    q.assemble_qvec(rho)
+    q.time_step_sys(qs, rho, 0.0, 1.0, 0.01, 1000)
+    n = q.get_expectation_value_qvec(rho, cav.n)
+
+Every call goes through the C ABI declared in include/quac_b200.h; the
+compute runs in the library's CUDA kernels.  There is no CPU fallback: on a
+machine without a GPU the compute calls fail with the CUDA error.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libquac_b200.so")
+
+# op_type, qvec_type, gate_type (include/quac_b200.h)
+RAISE, NUMBER, LOWER, VEC, SIGMA_X, SIGMA_Y, SIGMA_Z, IDENTITY, OTHER = -1, 0, 1, 2, 3, 4, 5, 6, 7
+DENSITY_MATRIX, WAVEFUNCTION = -1, 1
+GATES = dict(SQiSWP=-8, CZ_ARP=-7, CUSTOM2QGATE=-6, CZX=-5, CmZ=-4, CZ=-3, CXZ=-2, CNOT=-1,
+             HADAMARD=1, SIGMAX=2, SIGMAY=3, SIGMAZ=4, EYE=5, RX=6, RY=7, RZ=8, U1=9, U2=10,
+             U3=11, CUSTOM1QGATE=12)
+globals().update(GATES)
+_NQ = {g: (2 if v < 0 else 1) for g, v in GATES.items()}
+
+i64, dbl, vp = ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+
+
+class Scalar(ctypes.Structure):
+    """PetscScalar (complex double) passed by value."""
+    _fields_ = [("re", dbl), ("im", dbl)]
+
+
+def _sc(a):
+    a = complex(a)
+    return Scalar(a.real, a.imag)
+
+
+class _OpStruct(ctypes.Structure):
+    pass
+
+
+_OpPtr = ctypes.POINTER(_OpStruct)
+_OpStruct._fields_ = [
+    ("initial_pop", dbl), ("initial_exc", i64), ("n_before", i64), ("my_levels", i64),
+    ("my_op_type", ctypes.c_int), ("pos_in_sys_hspace", i64),
+    ("dag", _OpPtr), ("n", _OpPtr), ("sig_x", _OpPtr), ("sig_y", _OpPtr), ("sig_z", _OpPtr),
+    ("eye", _OpPtr), ("other", _OpPtr), ("position", i64), ("vec_op_list", vp),
+    ("evals", dbl * 4), ("evecs", dbl * 8)]
+
+
+class _QvecStruct(ctypes.Structure):
+    _fields_ = [("my_type", ctypes.c_int), ("ens_spawned", ctypes.c_int), ("n", i64),
+                ("Istart", i64), ("Iend", i64), ("total_levels", i64),
+                ("hspace_dims", ctypes.POINTER(i64)), ("ndims_hspace", i64), ("n_ops", i64),
+                ("n_ensemble", i64), ("ens_i", i64), ("data", vp), ("ens_datas", vp)]
+
+
+_MonitorFn = ctypes.CFUNCTYPE(ctypes.c_int, vp, i64, dbl, vp, vp)
+
+
+class _QsysStruct(ctypes.Structure):
+    _fields_ = [("num_time_indep", i64), ("num_time_dep", i64), ("hspace_frozen", i64),
+                ("dm_equations", ctypes.c_int), ("mcwf_solver", ctypes.c_int),
+                ("time_step_called", ctypes.c_int), ("mat_allocated", i64),
+                ("num_subsystems", i64), ("subsystem_list", ctypes.POINTER(_OpPtr)),
+                ("total_levels", i64), ("dim", i64), ("solution_qvec", vp), ("np", i64),
+                ("nid", i64), ("current_time", dbl), ("ts_monitor", vp), ("ts_ctx", vp),
+                ("num_circuits", i64), ("circuit_list_size", i64), ("current_circuit", i64),
+                ("circuit_list", vp), ("impl", vp)]
+
+
+class _GateStruct(ctypes.Structure):
+    _fields_ = [("time", dbl), ("run_time", dbl), ("my_gate_type", ctypes.c_int),
+                ("qubit_numbers", ctypes.POINTER(i64)), ("num_qubits", i64), ("custom_func", vp),
+                ("theta", dbl), ("phi", dbl), ("lambda_", dbl), ("gate_ctx", vp)]
+
+
+class _CircuitStruct(ctypes.Structure):
+    _fields_ = [("num_gates", i64), ("gate_list_size", i64), ("current_gate", i64),
+                ("num_layers", i64), ("current_layer", i64), ("start_time", dbl),
+                ("gate_list", ctypes.POINTER(_GateStruct)), ("layer_list", vp)]
+
+
+class CustomGateData(ctypes.Structure):
+    """custom_gate_data: a 4x4 complex matrix (row-major)."""
+    _fields_ = [("gate_data", dbl * 32)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libquac_b200.so (built in-tree by quac_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m quac_b200.build` first")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    sig = {
+        "QuaC_initialize": (None, [ctypes.c_int, vp]),
+        "QuaC_finalize": (None, []),
+        "initialize_system": (None, [P(P(_QsysStruct))]),
+        "destroy_system": (None, [P(P(_QsysStruct))]),
+        "create_op_sys": (None, [P(_QsysStruct), i64, P(_OpPtr)]),
+        "create_vec_op_sys": (None, [P(_QsysStruct), i64, P(P(_OpPtr))]),
+        "add_ham_term_list": (None, [P(_QsysStruct), Scalar, i64, P(_OpPtr)]),
+        "add_lin_term_list": (None, [P(_QsysStruct), Scalar, i64, P(_OpPtr)]),
+        "clear_mat_terms_sys": (None, [P(_QsysStruct)]),
+        "construct_matrix": (None, [P(_QsysStruct)]),
+        "time_step_sys": (None, [P(_QsysStruct), P(_QvecStruct), dbl, dbl, dbl, i64]),
+        "set_ts_monitor_sys": (None, [P(_QsysStruct), vp, vp]),
+        "set_init_excited_op": (None, [_OpPtr, i64]),
+        "set_qvec_from_init_excited_op": (None, [P(_QsysStruct), P(_QvecStruct)]),
+        "create_qvec_sys": (None, [P(_QsysStruct), P(P(_QvecStruct))]),
+        "create_dm_sys": (None, [P(_QsysStruct), P(P(_QvecStruct))]),
+        "create_wf_sys": (None, [P(_QsysStruct), P(P(_QvecStruct))]),
+        "create_arb_qvec": (None, [P(P(_QvecStruct)), i64, ctypes.c_int]),
+        "destroy_qvec": (None, [P(P(_QvecStruct))]),
+        "add_to_qvec_loc": (None, [P(_QvecStruct), Scalar, i64]),
+        "assemble_qvec": (None, [P(_QvecStruct)]),
+        "get_dm_element_qvec": (None, [P(_QvecStruct), i64, i64, P(Scalar)]),
+        "get_wf_element_qvec": (None, [P(_QvecStruct), i64, P(Scalar)]),
+        "get_trace_qvec": (None, [P(_QvecStruct), P(Scalar)]),
+        "get_expectation_value_qvec_list": (None, [P(_QvecStruct), P(Scalar), i64, P(_OpPtr)]),
+        "get_fidelity_qvec": (None, [P(_QvecStruct), P(_QvecStruct), P(dbl), P(dbl)]),
+        "copy_qvec": (None, [P(_QvecStruct), P(_QvecStruct)]),
+        "create_circuit": (None, [P(_CircuitStruct), i64]),
+        "destroy_circuit": (None, [P(_CircuitStruct)]),
+        "schedule_circuit_layers": (None, [P(_QsysStruct), P(_CircuitStruct)]),
+        "apply_circuit_to_sys": (None, [P(_QsysStruct), P(_CircuitStruct), dbl]),
+        "apply_circuit_to_qvec": (None, [P(_QsysStruct), _CircuitStruct, P(_QvecStruct)]),
+        "quac_add_gate": (ctypes.c_int, [P(_CircuitStruct), dbl, ctypes.c_int, ctypes.c_int,
+                                         P(ctypes.c_int), dbl, dbl, dbl, vp, vp]),
+        "quac_apply_gate": (ctypes.c_int, [P(_QvecStruct), ctypes.c_int, ctypes.c_int,
+                                           P(ctypes.c_int), dbl, dbl, dbl, vp]),
+        "steady_state_sys": (i64, [P(_QsysStruct), P(_QvecStruct)]),
+        "quac_lrho_apply_device": (ctypes.c_int, [P(_QsysStruct), vp, vp]),
+        "quac_lrho_apply_host": (ctypes.c_int, [P(_QsysStruct), vp, vp]),
+        "quac_time_step_host": (ctypes.c_int, [P(_QsysStruct), vp, dbl, dbl, dbl, i64]),
+        "quac_set_error_mode": (None, [ctypes.c_int]),
+        "quac_last_error": (ctypes.c_char_p, []),
+        "quac_clear_error": (None, []),
+        "quac_set_ts_options": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, dbl, dbl, i64]),
+        "quac_qvec_device_ptr": (vp, [P(_QvecStruct)]),
+        "quac_kernel_launch_count": (i64, []),
+        "quac_set_stream": (None, [P(_QsysStruct), vp]),
+        "VecGetSize": (ctypes.c_int, [vp, P(i64)]),
+        "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
+        "read_qvec_wf_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
+        "print_qvec_file": (None, [P(_QvecStruct), ctypes.c_char_p]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    L.quac_set_error_mode(1)  # errors come back as exceptions here
+    _lib = L
+    return L
+
+
+class QuacError(RuntimeError):
+    pass
+
+
+def _check():
+    msg = _lib.quac_last_error()
+    if msg:
+        _lib.quac_clear_error()
+        raise QuacError(msg.decode(errors="replace").strip())
+
+
+# ----------------------------------------------------------------- handles
+class Operator:
+    """A QuaC operator (op->dag, op->n, op->sig_x ... as attributes)."""
+
+    def __init__(self, ptr):
+        self._ptr = ptr
+
+    def _child(self, name):
+        p = getattr(self._ptr.contents, name)
+        return Operator(p) if p else None
+
+    @property
+    def dag(self):
+        return self._child("dag")
+
+    @property
+    def n(self):
+        return self._child("n")
+
+    @property
+    def eye(self):
+        return self._child("eye")
+
+    @property
+    def sig_x(self):
+        return self._child("sig_x")
+
+    @property
+    def sig_y(self):
+        return self._child("sig_y")
+
+    @property
+    def sig_z(self):
+        return self._child("sig_z")
+
+    @property
+    def other(self):
+        return self._child("other")
+
+    @property
+    def a(self):
+        return self
+
+    @property
+    def my_levels(self):
+        return self._ptr.contents.my_levels
+
+    @property
+    def n_before(self):
+        return self._ptr.contents.n_before
+
+    @property
+    def my_op_type(self):
+        return self._ptr.contents.my_op_type
+
+    @property
+    def position(self):
+        return self._ptr.contents.position
+
+    def triple(self, sub):
+        """(type, subsystem, position) as the oracle describes operators."""
+        return (self.my_op_type, sub, self.position)
+
+
+class QSystem:
+    def __init__(self, ptr):
+        self._ptr = ptr
+        self._monitor = None
+
+    @property
+    def dim(self):
+        return self._ptr.contents.dim
+
+    @property
+    def total_levels(self):
+        return self._ptr.contents.total_levels
+
+    @property
+    def dm_equations(self):
+        return bool(self._ptr.contents.dm_equations)
+
+    def destroy(self):
+        if self._ptr:
+            lib().destroy_system(ctypes.byref(self._ptr))
+            self._ptr = None
+
+
+class Qvec:
+    def __init__(self, ptr):
+        self._ptr = ptr
+
+    @property
+    def n(self):
+        return self._ptr.contents.n
+
+    @property
+    def my_type(self):
+        return self._ptr.contents.my_type
+
+    @property
+    def device_ptr(self):
+        return lib().quac_qvec_device_ptr(self._ptr)
+
+    def to_numpy(self):
+        """Copies the vector to host (column-stacked for a density matrix)."""
+        import ctypes as C
+        n = self.n
+        out = np.empty(n, dtype=np.complex128)
+        cudart = _cudart()
+        rc = cudart.cudaMemcpy(out.ctypes.data_as(C.c_void_p), C.c_void_p(self.device_ptr),
+                               C.c_size_t(16 * n), 2)
+        if rc != 0:
+            raise QuacError(f"cudaMemcpy failed ({rc})")
+        return out
+
+    def from_numpy(self, arr):
+        import ctypes as C
+        arr = np.ascontiguousarray(arr, dtype=np.complex128)
+        if arr.size != self.n:
+            raise ValueError("size mismatch")
+        cudart = _cudart()
+        rc = cudart.cudaMemcpy(C.c_void_p(self.device_ptr), arr.ctypes.data_as(C.c_void_p),
+                               C.c_size_t(16 * self.n), 1)
+        if rc != 0:
+            raise QuacError(f"cudaMemcpy failed ({rc})")
+
+    def destroy(self):
+        if self._ptr:
+            lib().destroy_qvec(ctypes.byref(self._ptr))
+            self._ptr = None
+
+
+_cudart_lib = None
+
+
+def _cudart():
+    global _cudart_lib
+    if _cudart_lib is None:
+        import glob
+        cands = glob.glob("/usr/local/cuda/lib64/libcudart.so*")
+        _cudart_lib = ctypes.CDLL(cands[0] if cands else "libcudart.so")
+        _cudart_lib.cudaMemcpy.restype = ctypes.c_int
+        _cudart_lib.cudaMemcpy.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_int]
+    return _cudart_lib
+
+
+# ------------------------------------------------------------- QuaC calls
+def QuaC_initialize(args=()):
+    argv = [b"quac"] + [a.encode() if isinstance(a, str) else a for a in args]
+    arr = (ctypes.c_char_p * (len(argv) + 1))(*argv, None)
+    lib().QuaC_initialize(len(argv), ctypes.cast(arr, vp))
+    _check()
+
+
+def QuaC_finalize():
+    lib().QuaC_finalize()
+
+
+def initialize_system():
+    p = ctypes.POINTER(_QsysStruct)()
+    lib().initialize_system(ctypes.byref(p))
+    _check()
+    return QSystem(p)
+
+
+def destroy_system(qs):
+    qs.destroy()
+
+
+def create_op_sys(qs, levels):
+    p = _OpPtr()
+    lib().create_op_sys(qs._ptr, int(levels), ctypes.byref(p))
+    _check()
+    return Operator(p)
+
+
+def create_vec_op_sys(qs, levels):
+    arr = ctypes.POINTER(_OpPtr)()
+    lib().create_vec_op_sys(qs._ptr, int(levels), ctypes.byref(arr))
+    _check()
+    return [Operator(arr[i]) for i in range(levels)]
+
+
+def _oplist(ops):
+    arr = (_OpPtr * max(1, len(ops)))(*[o._ptr for o in ops])
+    return arr
+
+
+def add_ham_term(qs, a, *ops):
+    lib().add_ham_term_list(qs._ptr, _sc(a), len(ops), _oplist(ops))
+    _check()
+
+
+def add_lin_term(qs, a, *ops):
+    lib().add_lin_term_list(qs._ptr, _sc(a), len(ops), _oplist(ops))
+    _check()
+
+
+def clear_mat_terms_sys(qs):
+    lib().clear_mat_terms_sys(qs._ptr)
+
+
+def construct_matrix(qs):
+    lib().construct_matrix(qs._ptr)
+    _check()
+
+
+def set_init_excited_op(op, exc):
+    lib().set_init_excited_op(op._ptr, int(exc))
+    _check()
+
+
+def set_qvec_from_init_excited_op(qs, q):
+    lib().set_qvec_from_init_excited_op(qs._ptr, q._ptr)
+    _check()
+
+
+def set_ts_options(rk_type="", adapt_type="", rtol=-1.0, atol=-1.0, max_steps=-1):
+    """Programmatic -ts_rk_type / -ts_adapt_type / -ts_rtol / -ts_atol / -ts_max_steps."""
+    lib().quac_set_ts_options(rk_type.encode(), adapt_type.encode(), rtol, atol, max_steps)
+    _check()
+
+
+def set_ts_monitor_sys(qs, fn):
+    """fn(step, time, vec_handle) called after each step (None clears)."""
+    if fn is None:
+        qs._monitor = None
+        lib().set_ts_monitor_sys(qs._ptr, None, None)
+        return
+
+    def _cb(ts, step, t, vec, ctx):
+        fn(step, t, vec)
+        return 0
+
+    qs._monitor = _MonitorFn(_cb)
+    lib().set_ts_monitor_sys(qs._ptr, ctypes.cast(qs._monitor, vp), None)
+
+
+def time_step_sys(qs, q, t0, tmax, dt, steps_max):
+    lib().time_step_sys(qs._ptr, q._ptr, float(t0), float(tmax), float(dt), int(steps_max))
+    _check()
+
+
+def create_qvec_sys(qs):
+    p = ctypes.POINTER(_QvecStruct)()
+    lib().create_qvec_sys(qs._ptr, ctypes.byref(p))
+    _check()
+    return Qvec(p)
+
+
+def create_dm_sys(qs):
+    p = ctypes.POINTER(_QvecStruct)()
+    lib().create_dm_sys(qs._ptr, ctypes.byref(p))
+    _check()
+    return Qvec(p)
+
+
+def create_wf_sys(qs):
+    p = ctypes.POINTER(_QvecStruct)()
+    lib().create_wf_sys(qs._ptr, ctypes.byref(p))
+    _check()
+    return Qvec(p)
+
+
+def create_arb_qvec(nstates, qtype):
+    p = ctypes.POINTER(_QvecStruct)()
+    lib().create_arb_qvec(ctypes.byref(p), int(nstates), int(qtype))
+    _check()
+    return Qvec(p)
+
+
+def destroy_qvec(q):
+    q.destroy()
+
+
+def add_to_qvec_loc(q, alpha, loc):
+    lib().add_to_qvec_loc(q._ptr, _sc(alpha), int(loc))
+    _check()
+
+
+def add_to_qvec(q, alpha, *locs):
+    """add_to_qvec(dm, a, col, row) adds at D*col + row; add_to_qvec(wf, a, i)."""
+    if q.my_type == DENSITY_MATRIX:
+        D = int(round(np.sqrt(q.n)))
+        add_to_qvec_loc(q, alpha, D * int(locs[0]) + int(locs[1]))
+    else:
+        add_to_qvec_loc(q, alpha, int(locs[0]))
+
+
+def assemble_qvec(q):
+    lib().assemble_qvec(q._ptr)
+    _check()
+
+
+def get_dm_element_qvec(q, row, col):
+    s = Scalar()
+    lib().get_dm_element_qvec(q._ptr, int(row), int(col), ctypes.byref(s))
+    _check()
+    return complex(s.re, s.im)
+
+
+def get_trace_qvec(q):
+    s = Scalar()
+    lib().get_trace_qvec(q._ptr, ctypes.byref(s))
+    _check()
+    return complex(s.re, s.im)
+
+
+def get_expectation_value_qvec(q, *ops):
+    s = Scalar()
+    lib().get_expectation_value_qvec_list(q._ptr, ctypes.byref(s), len(ops), _oplist(ops))
+    _check()
+    return complex(s.re, s.im)
+
+
+def get_fidelity_qvec(q1, q2):
+    f, v = dbl(), dbl()
+    lib().get_fidelity_qvec(q1._ptr, q2._ptr, ctypes.byref(f), ctypes.byref(v))
+    _check()
+    return f.value, v.value
+
+
+def copy_qvec(src, dst):
+    lib().copy_qvec(src._ptr, dst._ptr)
+    _check()
+
+
+class Circuit:
+    """The value struct `circuit` (create_circuit / add_gate_to_circuit_sys)."""
+
+    def __init__(self, num_gates):
+        self.c = _CircuitStruct()
+        self._ctx = []
+        lib().create_circuit(ctypes.byref(self.c), int(num_gates))
+
+    def add_gate(self, time, gate, *qubits, theta=0.0, phi=0.0, lam=0.0, ctx=None, func=None):
+        g = GATES[gate] if isinstance(gate, str) else int(gate)
+        qs = (ctypes.c_int * len(qubits))(*qubits)
+        if ctx is not None:
+            self._ctx.append(ctx)
+        rc = lib().quac_add_gate(ctypes.byref(self.c), float(time), g, len(qubits), qs, theta, phi,
+                                 lam, ctypes.cast(ctypes.pointer(ctx), vp) if ctx is not None else None,
+                                 ctypes.cast(func, vp) if func is not None else None)
+        _check()
+        return rc
+
+    def destroy(self):
+        lib().destroy_circuit(ctypes.byref(self.c))
+
+
+def create_circuit(num_gates):
+    return Circuit(num_gates)
+
+
+def add_gate_to_circuit_sys(circ, time, gate, *args, **kw):
+    """add_gate_to_circuit_sys(circ, t, 'RZ', q, theta) / (circ, t, 'U3', q, th, ph, la)."""
+    g = GATES[gate] if isinstance(gate, str) else int(gate)
+    name = gate if isinstance(gate, str) else [k for k, v in GATES.items() if v == g][0]
+    nq = _NQ[name]
+    qubits, params = args[:nq], args[nq:]
+    p = dict(theta=0.0, phi=0.0, lam=0.0)
+    if name in ("RX", "RY", "RZ"):
+        p["theta"] = params[0]
+    elif name in ("U1", "U2", "U3"):
+        p["theta"], p["phi"], p["lam"] = params
+    p.update(kw)
+    return circ.add_gate(time, g, *qubits, **p)
+
+
+def schedule_circuit_layers(qs, circ):
+    lib().schedule_circuit_layers(qs._ptr, ctypes.byref(circ.c))
+    _check()
+
+
+def apply_circuit_to_sys(qs, circ, time):
+    lib().apply_circuit_to_sys(qs._ptr, ctypes.byref(circ.c), float(time))
+    _check()
+
+
+def apply_circuit_to_qvec(qs, circ, q):
+    lib().apply_circuit_to_qvec(qs._ptr, circ.c, q._ptr)
+    _check()
+
+
+def apply_gate2(q, gate, *args, ctx=None):
+    """apply_gate2(q, 'CNOT', 0, 1) / (q, 'RZ', q0, theta) / (q, 'U3', q0, th, ph, la)."""
+    name = gate if isinstance(gate, str) else [k for k, v in GATES.items() if v == gate][0]
+    nq = _NQ[name]
+    qubits, params = args[:nq], list(args[nq:])
+    th = ph = la = 0.0
+    if name in ("RX", "RY", "RZ"):
+        th = params[0]
+    elif name in ("U1", "U2", "U3"):
+        th, ph, la = params
+    qa = (ctypes.c_int * nq)(*qubits)
+    lib().quac_apply_gate(q._ptr, GATES[name], nq, qa, th, ph, la,
+                          ctypes.cast(ctypes.pointer(ctx), vp) if ctx is not None else None)
+    _check()
+
+
+def steady_state_sys(qs, q):
+    its = lib().steady_state_sys(qs._ptr, q._ptr)
+    _check()
+    return its
+
+
+def lrho_apply_device(qs, x_ptr, y_ptr):
+    """y = L x on device buffers (qs.dim complex128 each)."""
+    lib().quac_lrho_apply_device(qs._ptr, vp(x_ptr), vp(y_ptr))
+    _check()
+
+
+def lrho_apply_host(qs, x):
+    """y = L x with host numpy arrays (copies in and out)."""
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    y = np.empty_like(x)
+    lib().quac_lrho_apply_host(qs._ptr, x.ctypes.data_as(vp), y.ctypes.data_as(vp))
+    _check()
+    return y
+
+
+def time_step_host(qs, x, t0, tmax, dt, steps_max):
+    """Integrates host data in place (H2D, integration, D2H in one call)."""
+    assert x.dtype == np.complex128 and x.flags.c_contiguous
+    lib().quac_time_step_host(qs._ptr, x.ctypes.data_as(vp), t0, tmax, dt, steps_max)
+    _check()
+    return x
+
+
+def kernel_launch_count():
+    return lib().quac_kernel_launch_count()
+
+
+def set_stream(qs, stream_ptr):
+    """Launch qs's kernels on a caller-owned CUDA stream (e.g. a torch stream's cuda_stream)."""
+    lib().quac_set_stream(qs._ptr, vp(stream_ptr) if stream_ptr else None)

@@ -1,0 +1,99 @@
+// Internal definitions shared by the host runtime and the CUDA kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "quac_b200.h"
+
+namespace quac {
+
+using cplx = std::complex<double>;
+
+// ---------------------------------------------------------------- errors
+// Records an error message; in EXIT mode prints it and exits like the
+// reference's PetscPrintf + exit() convention (e.g. qsystem.c:20-24).
+void fail(int exit_code, const char *fmt, ...);
+bool has_error();
+void check_cuda(cudaError_t e, const char *what, const char *file, int line);
+#define QCUDA(x) ::quac::check_cuda((x), #x, __FILE__, __LINE__)
+
+void count_launch(int n = 1);
+
+// ------------------------------------------------------------ device prog
+// Compiled form of the Lindblad terms of one qsystem (see terms.cpp).
+//   y[r,c] = (dr[r] + dc[c] + sum_t Jdrow_t[r] Jdcol_t[c]) x[r,c]
+//          + sum_t Lval_t[r] x[Lmap_t[r], c]                       left H terms
+//          + sum_t Rval_t[c] x[r, Rmap_t[c]]                       right H terms
+//          + sum_t Jrow_t[r] Jcol_t[c] x[Jmap_t[r], Jmap_t[c]]      jumps
+// Maps hold -1 where the operator row is empty.  Element (r,c) lives at
+// c*D + r (column stacking).  For a wavefunction, ncols = 1 and only the
+// left terms and dr are present.
+struct DevProg {
+  int D;
+  int ncols;
+  int nL, nR, nJ, nJd;
+  const int *Lmap;
+  const double2 *Lval;
+  const int *Rmap;
+  const double2 *Rval;
+  const int *Jmap;
+  const double2 *Jrow;
+  const double2 *Jcol;
+  const double2 *Jdrow;
+  const double2 *Jdcol;
+  const double2 *dr;
+  const double2 *dc;
+  // qubit fast path: every subsystem has two levels and every term is a
+  // one-qubit operator class the bit-mask kernel understands
+  int qubit_path;
+};
+
+// Host copy of the compiled terms (kept for the CPU-side checks and for
+// rebuilding the device program).
+struct HostProg {
+  int D = 0, ncols = 0;
+  std::vector<std::vector<int>> Lmap, Rmap, Jmap;
+  std::vector<std::vector<cplx>> Lval, Rval, Jrow, Jcol, Jdrow, Jdcol;
+  std::vector<cplx> dr, dc;
+};
+
+// Stage epilogue of the fused L.x kernel.  With K = (L x)[i]:
+//   kout[i]       = K                              (if kout)
+//   out_u[i]      = (base_u ? base_u[i] : 0) + coef_u * K   for u < nupd
+//   if nsum: the error-norm term (|e_i| / (atol + rtol*max(|y_i|,|yn_i|)))^2
+//   is accumulated into *nsum, with e_i the value of update `err_upd`,
+//   y_i = ny[i] and yn_i = nyn[i] (or the value of update `yn_upd` >= 0).
+struct Epi {
+  double2 *kout;
+  int nupd;
+  double2 *out[3];
+  const double2 *base[3];
+  double coef[3];
+  double *nsum;
+  int err_upd;
+  int yn_upd;
+  const double2 *ny;
+  const double2 *nyn;
+  double atol, rtol;
+};
+
+struct DeviceProgram {
+  DevProg dev{};
+  HostProg host;
+  std::vector<void *> allocations;
+  void release();
+};
+
+// Builds the device program of a qsystem's time-independent terms.
+// mode 0 = density matrix (L on D^2), 1 = Schroedinger (-iH on D).
+DeviceProgram *compile_terms(qsystem qs, int mode);
+
+// Kernel launchers (lrho.cu)
+void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t s);
+void zero_epi(Epi &e);
+
+}  // namespace quac

@@ -1,0 +1,261 @@
+// time_step_sys: explicit Runge-Kutta integration of d(rho)/dt = L rho with
+// every stage fused into one matrix-free L.x launch (lrho.cu).
+//
+// Replaces the PETSc TS set-up of qsystem.c:895-1098: TS_LINEAR with the
+// assembled Liouvillian as constant Jacobian, TSRK3BS by default,
+// atol = rtol = 5e-7, step limits [0.01, 1], final step matched to tmax,
+// the user monitor after every step, and circuit gates applied at their
+// event times (quantum_circuits.c:17-120).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "runtime.h"
+
+namespace quac {
+
+void apply_gate_superop(qsystem qs, const struct quantum_gate_struct &g, Vec v, bool is_dm,
+                        cudaStream_t s);
+void apply_gate_inplace(qvec q, const struct quantum_gate_struct &g, cudaStream_t s);
+
+namespace {
+
+struct Event {
+  double t;
+  int circ;
+  int idx;   // layer (scheduled) or gate (unscheduled) index
+  bool layer;
+};
+
+std::vector<Event> collect_events(qsystem qs, double t0, double tmax) {
+  std::vector<Event> ev;
+  for (PetscInt c = 0; c < qs->num_circuits; c++) {
+    circuit &C = qs->circuit_list[c];
+    if (C.num_layers > 0) {
+      for (PetscInt l = 0; l < C.num_layers; l++)
+        ev.push_back({C.layer_list[l].time + C.start_time, (int)c, (int)l, true});
+    } else {
+      for (PetscInt g = 0; g < C.num_gates; g++)
+        ev.push_back({C.gate_list[g].time + C.start_time, (int)c, (int)g, false});
+    }
+  }
+  std::stable_sort(ev.begin(), ev.end(), [](const Event &a, const Event &b) { return a.t < b.t; });
+  std::vector<Event> out;
+  for (auto &e : ev)
+    if (e.t > t0 && e.t <= tmax * (1 + 1e-14) + 1e-14) out.push_back(e);
+  return out;
+}
+
+// Stage helpers -------------------------------------------------------
+struct Stepper {
+  qsystem qs;
+  const DevProg *P;
+  cudaStream_t s;
+  int64_t n;
+  double atol, rtol;
+
+  void stage(const double2 *X, std::initializer_list<std::tuple<double2 *, const double2 *, double>> upd,
+             double *nsum = nullptr, int err_upd = 0, const double2 *ny = nullptr,
+             const double2 *nyn = nullptr) {
+    Epi e;
+    zero_epi(e);
+    int u = 0;
+    for (auto &t : upd) {
+      e.out[u] = std::get<0>(t);
+      e.base[u] = std::get<1>(t);
+      e.coef[u] = std::get<2>(t);
+      u++;
+    }
+    e.nupd = u;
+    e.nsum = nsum;
+    e.err_upd = err_upd;
+    e.ny = ny;
+    e.nyn = nyn;
+    e.atol = atol;
+    e.rtol = rtol;
+    launch_lrho(*P, X, e, s);
+  }
+};
+
+}  // namespace
+
+// Runs the integration on vector v (device-resident, length qs->dim).  The
+// qvec (if any) receives circuit gates and is handed to the monitor.
+int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int64_t steps_max) {
+  ensure_program(qs);
+  if (has_error() || !qs->impl->prog) return 1;
+  const DevProg &P = qs->impl->prog->dev;
+  const int64_t n = v->n;
+  if (n != (int64_t)P.D * P.ncols) {
+    fail(0, "ERROR! qvec size %ld does not match the system dimension %ld\n", (long)n,
+         (long)((int64_t)P.D * P.ncols));
+    return 1;
+  }
+  Options &o = options();
+  if (o.max_steps > 0) steps_max = o.max_steps;
+  const bool fixed = (o.rk_type == "4") || (o.adapt_type == "none");
+  const bool rk4 = (o.rk_type == "4");
+  cudaStream_t s = stream_of(qs);
+  Workspace &W = qs->impl->ws;
+  W.ensure(n, 4);
+  vec_sync_to_device(v);
+  QCUDA(cudaDeviceSynchronize());
+
+  Stepper st{qs, &P, s, n, o.atol, o.rtol};
+  std::vector<Event> events = x ? collect_events(qs, t0, tmax) : std::vector<Event>();
+  size_t next_ev = 0;
+  _p_TS ts;
+  ts.t = t0;
+  ts.dt = dt;
+  ts.step = 0;
+  if (qs->ts_monitor) qs->ts_monitor(&ts, 0, t0, v, qs->ts_ctx);
+
+  double t = t0, h = dt;
+  const double hmin = 0.01, hmax = 1.0;
+  int64_t steps = 0;
+  const double tend_tol = 1e-12 * std::max(1.0, std::fabs(tmax));
+  while (steps < steps_max && t < tmax - tend_tol && !has_error()) {
+    double h_try = h;
+    bool last = false;
+    if (t + h_try >= tmax - tend_tol) { h_try = tmax - t; last = true; }
+    bool at_event = false;
+    if (next_ev < events.size() && t + h_try >= events[next_ev].t - tend_tol) {
+      h_try = events[next_ev].t - t;
+      at_event = true;
+      last = false;
+      if (std::fabs(events[next_ev].t - tmax) <= tend_tol) last = true;
+    }
+    double2 *y = v->d;
+    bool accepted = true;
+    double h_next = h;
+    if (fixed && rk4) {
+      double2 *acc = W.bufs[0], *xa = W.bufs[1], *xb = W.bufs[2];
+      st.stage(y, {{acc, y, h_try / 6.0}, {xa, y, h_try / 2.0}});
+      st.stage(xa, {{acc, acc, h_try / 3.0}, {xb, y, h_try / 2.0}});
+      st.stage(xb, {{acc, acc, h_try / 3.0}, {xa, y, h_try}});
+      st.stage(xa, {{y, acc, h_try / 6.0}});
+    } else {
+      // Bogacki-Shampine 3(2): c = (0, 1/2, 3/4, 1), b = (2/9, 1/3, 4/9, 0),
+      // bhat = (7/24, 1/4, 1/3, 1/8); error = h * sum (b - bhat)_i k_i.
+      double2 *x1 = W.bufs[0], *x2 = W.bufs[1], *yn = W.bufs[2], *er = W.bufs[3];
+      st.stage(y, {{x1, y, 0.5 * h_try}, {yn, y, 2.0 / 9.0 * h_try}, {er, nullptr, (2.0 / 9.0 - 7.0 / 24.0) * h_try}});
+      st.stage(x1, {{x2, y, 0.75 * h_try}, {yn, yn, h_try / 3.0}, {er, er, (1.0 / 3.0 - 0.25) * h_try}});
+      st.stage(x2, {{yn, yn, 4.0 / 9.0 * h_try}, {er, er, (4.0 / 9.0 - 1.0 / 3.0) * h_try}});
+      if (fixed) {
+        std::swap(v->d, W.bufs[2]);
+      } else {
+        QCUDA(cudaMemsetAsync(W.dsum, 0, sizeof(double), s));
+        st.stage(yn, {{er, er, -0.125 * h_try}}, W.dsum, 0, y, yn);
+        QCUDA(cudaMemcpyAsync(W.hsum, W.dsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+        QCUDA(cudaStreamSynchronize(s));
+        const double err = std::sqrt(W.hsum[0] / (double)n);
+        double fac = err > 0 ? 0.9 * std::pow(err, -1.0 / 3.0) : 10.0;
+        fac = std::min(10.0, std::max(0.1, fac));
+        h_next = std::min(hmax, std::max(hmin, h_try * fac));
+        accepted = (err <= 1.0) || (h_try <= hmin * (1 + 1e-12));
+        if (accepted) std::swap(v->d, W.bufs[2]);
+        if (!accepted) { h = h_next; continue; }
+      }
+    }
+    steps++;
+    t = last ? tmax : t + h_try;
+    if (!fixed) h = h_next;
+    if (at_event && x) {
+      const double te = events[next_ev].t;
+      while (next_ev < events.size() && std::fabs(events[next_ev].t - te) <= tend_tol) {
+        const Event &e = events[next_ev];
+        circuit &C = qs->circuit_list[e.circ];
+        if (e.layer) {
+          gate_layer_struct &L = C.layer_list[e.idx];
+          for (PetscInt g = 0; g < L.num_gates; g++)
+            apply_gate_superop(qs, L.gate_list[g], v, x->my_type == DENSITY_MATRIX, s);
+          C.current_layer = e.idx + 1;
+        } else {
+          apply_gate_inplace(x, C.gate_list[e.idx], s);
+          C.current_gate = e.idx + 1;
+        }
+        next_ev++;
+      }
+    }
+    if (qs->ts_monitor) {
+      QCUDA(cudaStreamSynchronize(s));
+      ts.t = t;
+      ts.dt = h_try;
+      ts.step = steps;
+      qs->ts_monitor(&ts, steps, t, v, qs->ts_ctx);
+    }
+  }
+  QCUDA(cudaStreamSynchronize(s));
+  qs->current_time = t;
+  if (std::fabs(t - tmax) > 1e-8 && !has_error()) printf("ERROR! Did not reach final time! Reason: %d\n", -1);
+  return has_error() ? 1 : 0;
+}
+
+}  // namespace quac
+
+using namespace quac;
+
+extern "C" {
+
+void set_ts_monitor_sys(qsystem qs, quac_ts_monitor monitor, void *ctx) {
+  qs->ts_monitor = monitor;
+  qs->ts_ctx = ctx;
+}
+
+void time_step_sys(qsystem qs, qvec x, PetscReal t0, PetscReal tmax, PetscReal dt,
+                   PetscInt steps_max) {
+  qs->time_step_called = PETSC_TRUE;
+  qs->solution_qvec = x;
+  if (qs->mat_allocated != 1) {
+    fail(0, "ERROR! Matrix does not seem to be constructed! You need to\n       call construct_matrix!\n");
+    return;
+  }
+  integrate(qs, x, x->data, t0, tmax, dt, steps_max);
+}
+
+int quac_lrho_apply_device(qsystem qs, const void *x_dev, void *y_dev) {
+  if (qs->mat_allocated != 1) { fail(0, "ERROR! call construct_matrix first\n"); return 1; }
+  ensure_program(qs);
+  if (has_error()) return 1;
+  Epi e;
+  zero_epi(e);
+  e.kout = (double2 *)y_dev;
+  cudaStream_t s = stream_of(qs);
+  launch_lrho(qs->impl->prog->dev, (const double2 *)x_dev, e, s);
+  QCUDA(cudaStreamSynchronize(s));
+  return has_error() ? 1 : 0;
+}
+
+int quac_lrho_apply_host(qsystem qs, const PetscScalar *x_host, PetscScalar *y_host) {
+  if (qs->mat_allocated != 1) { fail(0, "ERROR! call construct_matrix first\n"); return 1; }
+  Workspace &W = qs->impl->ws;
+  const int64_t n = qs->dim;
+  W.ensure(n, 4);
+  cudaStream_t s = stream_of(qs);
+  QCUDA(cudaMemcpyAsync(W.bufs[0], x_host, n * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ensure_program(qs);
+  Epi e;
+  zero_epi(e);
+  e.kout = W.bufs[1];
+  launch_lrho(qs->impl->prog->dev, W.bufs[0], e, s);
+  QCUDA(cudaMemcpyAsync(y_host, W.bufs[1], n * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  QCUDA(cudaStreamSynchronize(s));
+  return has_error() ? 1 : 0;
+}
+
+int quac_time_step_host(qsystem qs, PetscScalar *x_host, PetscReal t0, PetscReal tmax,
+                        PetscReal dt, PetscInt steps_max) {
+  if (qs->mat_allocated != 1) { fail(0, "ERROR! call construct_matrix first\n"); return 1; }
+  const int64_t n = qs->dim;
+  Vec v = vec_new(n);
+  cudaStream_t s = stream_of(qs);
+  QCUDA(cudaMemcpyAsync(v->d, x_host, n * sizeof(double2), cudaMemcpyHostToDevice, s));
+  QCUDA(cudaStreamSynchronize(s));
+  int rc = integrate(qs, nullptr, v, t0, tmax, dt, steps_max);
+  QCUDA(cudaMemcpyAsync(x_host, v->d, n * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  QCUDA(cudaStreamSynchronize(s));
+  vec_free(v);
+  return rc;
+}
+
+}  // extern "C"

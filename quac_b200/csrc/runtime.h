@@ -1,0 +1,81 @@
+// Host-side runtime objects behind the opaque handles of quac_b200.h.
+#pragma once
+#include <map>
+#include <string>
+#include <vector>
+
+#include "common.h"
+
+// Vec: one complex128 vector in device memory with an on-demand host copy
+// (the VecGetArray stand-in maps it to host memory).
+struct _p_Vec {
+  int64_t n = 0;
+  double2 *d = nullptr;               // device data
+  std::vector<quac::cplx> h;          // host staging copy
+  bool host_pending = false;          // h holds additions not yet on the device
+  bool host_mapped = false;           // VecGetArray outstanding
+};
+
+struct _p_TS {
+  double t = 0, dt = 0;
+  int64_t step = 0;
+};
+
+namespace quac {
+
+struct Term {
+  int kind;  // 1 = Hamiltonian, 2 = Lindblad
+  cplx a;
+  std::vector<op_handle> ops;
+};
+
+struct Options {
+  std::string rk_type = "3bs";
+  std::string adapt_type = "basic";
+  double rtol = 5e-7, atol = 5e-7;  // qsystem.c:902
+  int64_t max_steps = -1;           // -1: use the caller's steps_max
+  bool rtol_set = false, atol_set = false;
+};
+Options &options();
+
+// Workspace of one integrator (device buffers of dim complex128 each).
+struct Workspace {
+  int64_t dim = 0;
+  std::vector<double2 *> bufs;
+  double *dsum = nullptr;   // device scalars
+  double *hsum = nullptr;   // pinned host mirror
+  void ensure(int64_t dim, int nbufs);
+  void release();
+};
+
+}  // namespace quac
+
+struct qsystem_impl {
+  std::vector<quac::Term> terms;
+  quac::DeviceProgram *prog = nullptr;
+  int prog_mode = -1;
+  cudaStream_t stream = nullptr;       // owned
+  cudaStream_t user_stream = nullptr;  // set by quac_set_stream (not owned)
+  quac::Workspace ws;
+  std::vector<op_handle> owned_ops;  // every operator struct created for this system
+};
+
+namespace quac {
+cudaStream_t stream_of(qsystem qs);
+void ensure_program(qsystem qs);
+int64_t vec_len(Vec v);
+void vec_sync_to_device(Vec v);       // flush pending host additions
+Vec vec_new(int64_t n);
+void vec_free(Vec v);
+// Observable kernels (observe.cu)
+cplx dm_expectation(const double2 *rho, int64_t D, const int *colmap, const double2 *colval,
+                    cudaStream_t s);
+cplx wf_expectation(const double2 *psi, int64_t D, const int *map, const double2 *val,
+                    cudaStream_t s);
+cplx dm_trace(const double2 *rho, int64_t D, cudaStream_t s);
+double dm_wf_fidelity(const double2 *rho, const double2 *psi, int64_t D, cudaStream_t s);
+cplx vdot(const double2 *a, const double2 *b, int64_t n, cudaStream_t s);
+// Operator-product row map on the Hilbert space (terms.cpp)
+void op_chain_map(int64_t D, const std::vector<op_handle> &ops, std::vector<int> &map,
+                  std::vector<cplx> &val);
+}  // namespace quac

@@ -1,0 +1,296 @@
+// Steady state: solve (L + e0 vec(I)^T) x = e0 by restarted GMRES on the
+// GPU (solver.c:33-221 does the same system with PETSc KSPGMRES(100),
+// rtol 1e-11, x0 = b = e0; row 0 carries the trace functional,
+// solver.c:60-75).
+//
+// Every vector operation runs on device buffers; the Krylov basis V is one
+// (m+1) x n block so the Gram-Schmidt projections are two streaming
+// kernels per pass (multi-dot, multi-axpy), repeated once (CGS2).  Only the
+// (m+1) x m Hessenberg matrix lives on the host.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "runtime.h"
+
+namespace quac {
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int CHUNK = 1024;  // elements of w staged per block
+
+__device__ __forceinline__ double2 cmuls(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+
+// y[0] += sum_i x[i*(D+1)]  (the stabilising trace row)
+__global__ void k_trace_add(const double2 *__restrict__ x, double2 *__restrict__ y, int64_t D) {
+  __shared__ double2 red[NT / 32];
+  double2 acc = make_double2(0.0, 0.0);
+  for (int64_t i = threadIdx.x; i < D; i += NT) {
+    const double2 v = x[i * (D + 1)];
+    acc.x += v.x; acc.y += v.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double2 s = make_double2(0.0, 0.0);
+    for (int w = 0; w < NT / 32; w++) { s.x += red[w].x; s.y += red[w].y; }
+    y[0].x += s.x;
+    y[0].y += s.y;
+  }
+}
+
+// partial[k*nb + blk] = sum over this block's chunk of conj(V_k[i]) w[i]
+__global__ void k_multidot(const double2 *__restrict__ V, const double2 *__restrict__ w, int64_t n,
+                           int nk, double2 *__restrict__ partial) {
+  __shared__ double2 ws[CHUNK];
+  __shared__ double2 red[2][NT / 32];
+  const int64_t i0 = (int64_t)blockIdx.x * CHUNK;
+  const int len = (int)min((int64_t)CHUNK, n - i0);
+  for (int i = threadIdx.x; i < len; i += NT) ws[i] = w[i0 + i];
+  __syncthreads();
+  for (int k = 0; k < nk; k++) {
+    const double2 *vk = V + (size_t)k * n + i0;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int i = threadIdx.x; i < len; i += NT) {
+      double2 a = vk[i];
+      a.y = -a.y;
+      const double2 p = cmuls(a, ws[i]);
+      acc.x += p.x; acc.y += p.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+      acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) red[k & 1][threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double2 s = make_double2(0.0, 0.0);
+      for (int q = 0; q < NT / 32; q++) { s.x += red[k & 1][q].x; s.y += red[k & 1][q].y; }
+      partial[(size_t)k * gridDim.x + blockIdx.x] = s;
+    }
+  }
+}
+
+// h[k] (+)= sum_b partial[k*nb + b]; one block per k.  accumulate != 0 adds.
+__global__ void k_reduce_rows(const double2 *__restrict__ partial, int nb, double2 *__restrict__ h,
+                              int accumulate) {
+  __shared__ double2 red[NT / 32];
+  const int k = blockIdx.x;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int b = threadIdx.x; b < nb; b += NT) {
+    acc.x += partial[(size_t)k * nb + b].x;
+    acc.y += partial[(size_t)k * nb + b].y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double2 s = make_double2(0.0, 0.0);
+    for (int q = 0; q < NT / 32; q++) { s.x += red[q].x; s.y += red[q].y; }
+    if (accumulate) { h[k].x += s.x; h[k].y += s.y; }
+    else h[k] = s;
+  }
+}
+
+// w[i] -= sum_k c[k] V_k[i]   (c = the projections just computed)
+__global__ void k_multiaxpy(const double2 *__restrict__ V, const double2 *__restrict__ c, int64_t n,
+                            int nk, double2 *__restrict__ w, double sign) {
+  __shared__ double2 cs[128];
+  for (int k = threadIdx.x; k < nk; k += NT) cs[k] = c[k];
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    double2 acc = w[i];
+    for (int k = 0; k < nk; k++) {
+      const double2 p = cmuls(cs[k], V[(size_t)k * n + i]);
+      acc.x = fma(sign, p.x, acc.x);
+      acc.y = fma(sign, p.y, acc.y);
+    }
+    w[i] = acc;
+  }
+}
+
+// out = in * s (s real), returns nothing; also used to copy (s = 1)
+__global__ void k_scale(const double2 *__restrict__ in, double2 *__restrict__ out, int64_t n, double s) {
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    const double2 v = in[i];
+    out[i] = make_double2(v.x * s, v.y * s);
+  }
+}
+
+// r = e0 - r
+__global__ void k_e0_minus(double2 *__restrict__ r, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    double2 v = r[i];
+    v.x = (i == 0 ? 1.0 : 0.0) - v.x;
+    v.y = -v.y;
+    r[i] = v;
+  }
+}
+
+int grid_for(int64_t n) {
+  int64_t b = (n + NT - 1) / NT;
+  return (int)std::min<int64_t>(b, 148 * 8);
+}
+
+}  // namespace
+
+// GMRES state bound to one qsystem (buffers reused across solves).
+struct Gmres {
+  int m = 0;
+  int64_t n = 0;
+  double2 *V = nullptr;        // (m+1) x n
+  double2 *w = nullptr;
+  double2 *partial = nullptr;  // (m+1) x nb
+  double2 *h = nullptr;        // m+1 projections
+  double2 *hh = nullptr;       // pinned host copy
+  int nb = 0;
+  void ensure(int64_t n_, int m_) {
+    if (n_ == n && m_ == m) return;
+    release();
+    n = n_;
+    m = m_;
+    nb = (int)((n + CHUNK - 1) / CHUNK);
+    QCUDA(cudaMalloc(&V, (size_t)(m + 1) * n * sizeof(double2)));
+    QCUDA(cudaMalloc(&w, (size_t)n * sizeof(double2)));
+    QCUDA(cudaMalloc(&partial, (size_t)(m + 1) * nb * sizeof(double2)));
+    QCUDA(cudaMalloc(&h, (size_t)(m + 1) * sizeof(double2)));
+    QCUDA(cudaMallocHost(&hh, (size_t)(m + 1) * sizeof(double2)));
+  }
+  void release() {
+    if (V) { cudaFree(V); cudaFree(w); cudaFree(partial); cudaFree(h); cudaFreeHost(hh); }
+    V = w = partial = h = hh = nullptr;
+    n = 0;
+    m = 0;
+  }
+};
+
+static Gmres &gmres_for(qsystem) {
+  static Gmres g;  // one solver workspace per process
+  return g;
+}
+
+// A x with A = L + e0 vec(I)^T
+static void apply_A(const DevProg &P, const double2 *x, double2 *y, cudaStream_t s) {
+  Epi e;
+  zero_epi(e);
+  e.kout = y;
+  launch_lrho(P, x, e, s);
+  k_trace_add<<<1, NT, 0, s>>>(x, y, P.D);
+  count_launch();
+}
+
+static double norm2(const double2 *x, int64_t n, cudaStream_t s) {
+  return std::sqrt(std::max(0.0, vdot(x, x, n, s).real()));
+}
+
+// Returns iterations, fills x (device, length n).  rtol is relative to ||b|| = 1.
+int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, bool x_is_guess,
+                    double *final_res) {
+  ensure_program(qs);
+  const DevProg &P = qs->impl->prog->dev;
+  const int64_t n = (int64_t)P.D * P.ncols;
+  cudaStream_t s = stream_of(qs);
+  if (m < 1 || m > 127) { fail(9, "ERROR! GMRES restart must be in [1, 127]\n"); return -1; }
+  Gmres &G = gmres_for(qs);
+  G.ensure(n, m);
+  if (!x_is_guess) {
+    QCUDA(cudaMemsetAsync(x, 0, n * sizeof(double2), s));
+    const double2 one = make_double2(1.0, 0.0);
+    QCUDA(cudaMemcpyAsync(x, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
+  }
+  std::vector<std::complex<double>> H((size_t)(m + 1) * m), cs(m), sn(m), gvec(m + 1), y(m);
+  int64_t it = 0;
+  double res = 0;
+  while (true) {
+    // r = b - A x  -> V_0
+    apply_A(P, x, G.V, s);
+    k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.V, n);
+    count_launch();
+    const double beta = norm2(G.V, n, s);
+    res = beta;
+    if (beta <= rtol || it >= maxit) break;
+    k_scale<<<grid_for(n), NT, 0, s>>>(G.V, G.V, n, 1.0 / beta);
+    count_launch();
+    std::fill(gvec.begin(), gvec.end(), 0.0);
+    gvec[0] = beta;
+    int j = 0;
+    bool conv = false;
+    for (; j < m && it < maxit; j++, it++) {
+      apply_A(P, G.V + (size_t)j * n, G.w, s);
+      // CGS2 with the projections summed on the host
+      std::vector<std::complex<double>> hsum(j + 1, 0.0);
+      for (int pass = 0; pass < 2; pass++) {
+        k_multidot<<<G.nb, NT, 0, s>>>(G.V, G.w, n, j + 1, G.partial);
+        k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, G.h, 0);
+        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j + 1, G.w, -1.0);
+        count_launch(3);
+        QCUDA(cudaMemcpyAsync(G.hh, G.h, (j + 1) * sizeof(double2), cudaMemcpyDeviceToHost, s));
+        QCUDA(cudaStreamSynchronize(s));
+        for (int k = 0; k <= j; k++) hsum[k] += std::complex<double>(G.hh[k].x, G.hh[k].y);
+      }
+      const double hn = norm2(G.w, n, s);
+      for (int k = 0; k <= j; k++) H[(size_t)k * m + j] = hsum[k];
+      H[(size_t)(j + 1) * m + j] = hn;
+      if (hn > 0) {
+        k_scale<<<grid_for(n), NT, 0, s>>>(G.w, G.V + (size_t)(j + 1) * n, n, 1.0 / hn);
+        count_launch();
+      }
+      for (int k = 0; k < j; k++) {
+        auto a = H[(size_t)k * m + j], b = H[(size_t)(k + 1) * m + j];
+        H[(size_t)k * m + j] = std::conj(cs[k]) * a + std::conj(sn[k]) * b;
+        H[(size_t)(k + 1) * m + j] = -sn[k] * a + cs[k] * b;
+      }
+      auto a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+      const double r = std::sqrt(std::norm(a) + std::norm(b));
+      if (r == 0) { cs[j] = 1; sn[j] = 0; }
+      else { cs[j] = a / r; sn[j] = b / r; }
+      H[(size_t)j * m + j] = r;
+      H[(size_t)(j + 1) * m + j] = 0;
+      gvec[j + 1] = -sn[j] * gvec[j];
+      gvec[j] = std::conj(cs[j]) * gvec[j];
+      if (std::abs(gvec[j + 1]) <= rtol || hn == 0) { j++; it++; conv = true; break; }
+    }
+    // solve the triangular system and update x += V y
+    for (int k = j - 1; k >= 0; k--) {
+      auto sum = gvec[k];
+      for (int q = k + 1; q < j; q++) sum -= H[(size_t)k * m + q] * y[q];
+      y[k] = sum / H[(size_t)k * m + k];
+    }
+    if (j > 0) {
+      std::vector<double2> yh(j);
+      for (int k = 0; k < j; k++) yh[k] = make_double2(y[k].real(), y[k].imag());
+      QCUDA(cudaMemcpyAsync(G.h, yh.data(), j * sizeof(double2), cudaMemcpyHostToDevice, s));
+      k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j, x, 1.0);
+      count_launch();
+      QCUDA(cudaStreamSynchronize(s));
+    }
+    (void)conv;
+  }
+  QCUDA(cudaStreamSynchronize(s));
+  if (final_res) *final_res = res;
+  return it;
+}
+
+}  // namespace quac
+
+using namespace quac;
+
+extern "C" PetscInt steady_state_sys(qsystem qs, qvec x) {
+  if (!qs->dm_equations) { fail(0, "ERROR! steady_state_sys needs Lindblad terms\n"); return -1; }
+  if (!qs->mat_allocated) construct_matrix(qs);
+  if (has_error()) return -1;
+  vec_sync_to_device(x->data);
+  double res = 0;
+  const int64_t its = gmres_solve(qs, x->data->d, 1e-11, 100, 200000, false, &res);
+  return has_error() ? -1 : its;
+}

@@ -1,0 +1,288 @@
+"""CUDA path against the oracle (run on a B200: pytest -m gpu).
+
+Tolerances: complex128 arithmetic throughout; the matrix-free kernel sums
+the same products as the assembled CSR in a different order, so results
+agree to ~1e-14 relative.  The bar in these tests is 1e-12 relative for one
+L.x, 1e-10 relative for integrated states, 1e-12 for
+gates and observables.
+"""
+import numpy as np
+import pytest
+
+import fixture_systems as F
+import helpers as H
+from conftest import golden_csr
+
+pytestmark = pytest.mark.gpu
+
+
+def _lrho(q, S, x):
+    q.construct_matrix(S.qs)
+    return q.lrho_apply_host(S.qs, x)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("case", F.CASES, ids=lambda c: f"{c[0]}-{c[1]}op-{c[2]}-{'c' if c[3] else 'r'}")
+def test_lrho_matches_golden_fixture(quac, golden, case):
+    fam, nop, kind, cplx = case
+    S = H.ProductSystem(quac)
+    stems = F.build(S, fam, nop, kind, cplx)
+    ref = sum(golden_csr(golden, s) for s in stems)
+    x = np.random.default_rng(7).normal(size=ref.shape[0]) + 1j * np.random.default_rng(8).normal(size=ref.shape[0])
+    y = _lrho(quac, S, x)
+    assert _rel(y, ref @ x) < 1e-12
+    S.qs.destroy()
+
+
+@pytest.mark.parametrize("build", [
+    lambda S: H.jc(S),
+    lambda S: H.driven_jc(S, 13, 0.2, 0.1, 0.3, 0.05),
+    lambda S: H.tfim(S, 6),
+    lambda S: H.tfim(S, 8),
+    lambda S: H.tavis_cummings(S, ne=3, nc=5),
+    lambda S: H.mixed(S),
+], ids=["jc", "driven_jc13", "tfim6", "tfim8", "tc3x5", "mixed3x2x5"])
+def test_lrho_matches_oracle(quac, oracle, build):
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    build(S)
+    build(O)
+    A = O.liouvillian()
+    for seed in range(2):
+        x = H.random_state(S.D, seed=seed)
+        y = _lrho(quac, S, x)
+        assert _rel(y, A @ x) < 1e-12
+    S.qs.destroy()
+
+
+def test_lrho_device_entry_point(quac, oracle):
+    import torch
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.tfim(S, 7)
+    H.tfim(O, 7)
+    quac.construct_matrix(S.qs)
+    x = H.random_state(S.D, seed=3)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    quac.lrho_apply_device(S.qs, xd.data_ptr(), yd.data_ptr())
+    torch.cuda.synchronize()
+    assert _rel(yd.cpu().numpy(), O.liouvillian() @ x) < 1e-12
+    S.qs.destroy()
+
+
+def test_rk4_fixed_step_matches_oracle(quac, oracle):
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    qb, cav = H.jc(S)
+    H.jc(O)
+    quac.construct_matrix(S.qs)
+    rho = quac.create_qvec_sys(S.qs)
+    quac.add_to_qvec(rho, 1.0, 10, 10)
+    quac.assemble_qvec(rho)
+    quac.set_ts_options(rk_type="4", adapt_type="none")
+    try:
+        quac.time_step_sys(S.qs, rho, 0.0, 2.0, 0.01, 100000)
+    finally:
+        quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+    y = rho.to_numpy()
+    h = O.csr_handle()
+    x0 = np.zeros(400, dtype=complex)
+    x0[10 * 20 + 10] = 1.0
+    yo = oracle.rk4(h, x0, 0.01, 200)
+    oracle.free_csr(h)
+    assert _rel(y, yo) < 1e-10
+    n_q = quac.get_expectation_value_qvec(rho, qb.n)
+    assert abs(n_q - oracle.expect_dm([2, 10], yo, (0, 0, -1))) < 1e-12
+    rho.destroy()
+    S.qs.destroy()
+
+
+def test_bs3_adaptive_matches_oracle(quac, oracle):
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.driven_jc(S, 8, 0.3, 0.2, 0.1, 0.05)
+    H.driven_jc(O, 8, 0.3, 0.2, 0.1, 0.05)
+    quac.construct_matrix(S.qs)
+    rho = quac.create_qvec_sys(S.qs)
+    D = S.D
+    quac.add_to_qvec(rho, 1.0, 8, 8)
+    quac.assemble_qvec(rho)
+    quac.time_step_sys(S.qs, rho, 0.0, 3.0, 0.05, 100000)
+    y = rho.to_numpy()
+    h = O.csr_handle()
+    x0 = np.zeros(D * D, dtype=complex)
+    x0[8 * D + 8] = 1.0
+    yo, nacc, nrej = oracle.bs3(h, x0, 0.0, 3.0, 0.05)
+    oracle.free_csr(h)
+    assert _rel(y, yo) < 1e-10
+    rho.destroy()
+    S.qs.destroy()
+
+
+def test_t1_decay_known_answer_gpu(quac):
+    q = quac
+    qs = q.initialize_system()
+    vop = q.create_vec_op_sys(qs, 2)
+    q.add_lin_term(qs, 1.0, vop[0], vop[1])
+    dm = q.create_qvec_sys(qs)
+    q.add_to_qvec(dm, 1.0, 1, 1)
+    q.assemble_qvec(dm)
+    q.construct_matrix(qs)
+    q.time_step_sys(qs, dm, 0.0, 1.0, 0.05, 200)
+    v = q.get_expectation_value_qvec(dm, vop[1], vop[1])
+    assert abs(v.real - np.exp(-1)) < 1e-4
+    dm.destroy()
+    qs.destroy()
+
+
+def test_circuit_events_during_time_step(quac):
+    """time_step_tests.c:337-396: unscheduled circuit gates use in-place
+    qubit numbering (qubit 0 = last subsystem)."""
+    q = quac
+    qs = q.initialize_system()
+    op2 = q.create_op_sys(qs, 2)
+    op3 = q.create_op_sys(qs, 2)
+    q.add_ham_term(qs, 1.0, op2.n)
+    q.add_lin_term(qs, 1.0, op2)
+    q.add_lin_term(qs, 1.0, op3)
+    dm = q.create_qvec_sys(qs)
+    q.add_to_qvec(dm, 1.0, 0, 0)
+    q.assemble_qvec(dm)
+    q.construct_matrix(qs)
+    circ = q.create_circuit(5)
+    q.add_gate_to_circuit_sys(circ, 0.0, "SIGMAX", 0)
+    q.add_gate_to_circuit_sys(circ, 0.1, "SIGMAX", 1)
+    q.apply_circuit_to_sys(qs, circ, 0.1)
+    q.time_step_sys(qs, dm, 0.0, 1.1, 0.05, 200)
+    assert abs(q.get_expectation_value_qvec(dm, op2.n).real - np.exp(-0.9)) < 5e-4
+    assert abs(q.get_expectation_value_qvec(dm, op3.n).real - np.exp(-1.0)) < 5e-4
+    dm.destroy()
+    qs.destroy()
+
+
+GATE_CASES = [("HADAMARD", [1], {}), ("SIGMAX", [2], {}), ("SIGMAY", [0], {}), ("SIGMAZ", [1], {}),
+              ("EYE", [0], {}), ("RX", [2], dict(theta=0.37)), ("RY", [1], dict(theta=-1.2)),
+              ("RZ", [0], dict(theta=2.1)), ("U3", [1], dict(theta=0.4, phi=1.3, lam=-0.8)),
+              ("U2", [2], dict(theta=np.pi / 2, phi=0.2, lam=0.9)),
+              ("U1", [0], dict(theta=0.0, phi=0.0, lam=0.6)),
+              ("CNOT", [0, 2], {}), ("CNOT", [2, 0], {}), ("CXZ", [1, 0], {}), ("CZX", [0, 1], {}),
+              ("CZ", [2, 1], {}), ("CmZ", [1, 2], {}), ("CZ_ARP", [0, 2], {})]
+
+
+@pytest.mark.parametrize("gate,qubits,kw", GATE_CASES, ids=lambda v: str(v))
+def test_superop_gate_matches_oracle(quac, oracle, gate, qubits, kw):
+    q = quac
+    qs = q.initialize_system()
+    for _ in range(3):
+        q.create_op_sys(qs, 2)
+    dm = q.create_dm_sys(qs)
+    x = H.random_state(8, seed=11)
+    dm.from_numpy(x)
+    c = q.create_circuit(1)
+    c.add_gate(0.0, gate, *qubits, theta=kw.get("theta", 0.0), phi=kw.get("phi", 0.0),
+               lam=kw.get("lam", 0.0))
+    q.apply_circuit_to_qvec(qs, c, dm)
+    ref = oracle.gate_superop([2, 2, 2], x, gate, qubits, **kw)
+    assert _rel(dm.to_numpy(), ref) < 1e-12
+    dm.destroy()
+    qs.destroy()
+
+
+INPLACE_CASES = [("HADAMARD", [1], {}), ("SIGMAX", [2], {}), ("RZ", [0], dict(theta=0.8)),
+                 ("U3", [2], dict(theta=0.4, phi=1.3, lam=-0.8)), ("CNOT", [0, 2], {}),
+                 ("CNOT", [2, 1], {}), ("CZ_ARP", [1, 2], {}), ("SQiSWP", [0, 1], {})]
+
+
+@pytest.mark.parametrize("gate,qubits,kw", INPLACE_CASES, ids=lambda v: str(v))
+def test_inplace_gate_matches_oracle(quac, oracle, gate, qubits, kw):
+    q = quac
+    qs = q.initialize_system()
+    for _ in range(3):
+        q.create_op_sys(qs, 2)
+    dm = q.create_dm_sys(qs)
+    x = H.random_state(8, seed=12)
+    dm.from_numpy(x)
+    args = list(qubits)
+    if gate == "RZ":
+        args.append(kw["theta"])
+    if gate == "U3":
+        args += [kw["theta"], kw["phi"], kw["lam"]]
+    q.apply_gate2(dm, gate, *args)
+    ref = oracle.gate_inplace([2] * 6, x, gate, qubits, **kw)
+    assert _rel(dm.to_numpy(), ref) < 1e-12
+    dm.destroy()
+    qs.destroy()
+
+
+def test_observables_match_numpy(quac, oracle):
+    q = quac
+    S = H.ProductSystem(q)
+    a, b, c = H.mixed(S)
+    dm = q.create_dm_sys(S.qs)
+    D = S.D
+    x = H.random_state(D, seed=5, hermitian=True)
+    dm.from_numpy(x)
+    for ops, trip in [((c.n,), [(0, 2, -1)]), ((a.dag, c.a), [(-1, 0, -1), (1, 2, -1)]),
+                      ((b.sig_x,), [(3, 1, -1)])]:
+        got = q.get_expectation_value_qvec(dm, *ops)
+        ref = oracle.expect_dm(S.levels, x, *trip)
+        assert abs(got - ref) < 1e-12
+    assert abs(q.get_trace_qvec(dm) - np.trace(x.reshape(D, D, order="F"))) < 1e-12
+    wf = q.create_arb_qvec(D, q.WAVEFUNCTION)
+    psi = np.random.default_rng(3).normal(size=D) + 1j * np.random.default_rng(4).normal(size=D)
+    psi /= np.linalg.norm(psi)
+    wf.from_numpy(psi)
+    f, _ = q.get_fidelity_qvec(dm, wf)
+    R = x.reshape(D, D, order="F")
+    assert abs(f - (psi.conj() @ R @ psi).real) < 1e-12
+    dm.destroy()
+    wf.destroy()
+    S.qs.destroy()
+
+
+def test_steady_state_matches_direct_solve(quac, oracle):
+    import scipy.sparse.linalg as sla
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.tavis_cummings(S, ne=2, nc=4)
+    H.tavis_cummings(O, ne=2, nc=4)
+    quac.construct_matrix(S.qs)
+    x = quac.create_qvec_sys(S.qs)
+    its = quac.steady_state_sys(S.qs, x)
+    assert its > 0
+    D = S.D
+    A = O.liouvillian().tolil()
+    for i in range(D):
+        A[0, i * (D + 1)] += 1.0
+    b = np.zeros(D * D, dtype=complex)
+    b[0] = 1
+    xd = sla.spsolve(A.tocsr(), b)
+    assert _rel(x.to_numpy(), xd) < 1e-9
+    x.destroy()
+    S.qs.destroy()
+
+
+def test_monitor_called_every_step(quac):
+    q = quac
+    S = H.ProductSystem(q)
+    qb, cav = H.jc(S, nc=4)
+    q.construct_matrix(S.qs)
+    rho = q.create_qvec_sys(S.qs)
+    q.add_to_qvec(rho, 1.0, 4, 4)
+    q.assemble_qvec(rho)
+    seen = []
+    q.set_ts_monitor_sys(S.qs, lambda step, t, vec: seen.append((step, t)))
+    q.set_ts_options(rk_type="4", adapt_type="none")
+    try:
+        q.time_step_sys(S.qs, rho, 0.0, 0.1, 0.01, 1000)
+    finally:
+        q.set_ts_options(rk_type="3bs", adapt_type="basic")
+        q.set_ts_monitor_sys(S.qs, None)
+    assert [s for s, _ in seen] == list(range(11))
+    assert abs(seen[-1][1] - 0.1) < 1e-12
+    rho.destroy()
+    S.qs.destroy()

@@ -163,6 +163,7 @@ def lib():
         "quac_qvec_device_ptr": (vp, [P(_QvecStruct)]),
         "quac_kernel_launch_count": (i64, []),
         "quac_set_stream": (None, [P(_QsysStruct), vp]),
+        "quac_set_kernel_path": (None, [ctypes.c_int]),
         "VecGetSize": (ctypes.c_int, [vp, P(i64)]),
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "read_qvec_wf_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
@@ -624,3 +625,8 @@ def kernel_launch_count():
 def set_stream(qs, stream_ptr):
     """Launch qs's kernels on a caller-owned CUDA stream (e.g. a torch stream's cuda_stream)."""
     lib().quac_set_stream(qs._ptr, vp(stream_ptr) if stream_ptr else None)
+
+
+def set_kernel_path(path):
+    """0: bit-mask kernel for all-qubit systems (default); 1: generic kernel only."""
+    lib().quac_set_kernel_path(int(path))

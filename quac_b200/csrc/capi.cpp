@@ -1174,3 +1174,7 @@ int quac_apply_gate(qvec q, int t, int nq, const int *qubits, double th, double 
 extern "C" void quac_set_stream(qsystem qs, void *stream) {
   qs->impl->user_stream = (cudaStream_t)stream;
 }
+
+extern "C" void quac_set_kernel_path(int path) {
+  options().kernel_path = path;
+}

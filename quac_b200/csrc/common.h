@@ -81,9 +81,34 @@ struct Epi {
   double atol, rtol;
 };
 
+// Qubit fast path: every subsystem is two-level, so each operator product
+// is, per qubit, a flip / condition / sign and the whole term is
+//   w(r) = coef * (-1)^popc(r & smask)   if (r & cmask) == cval, else 0,
+//   partner r ^ fmask
+// on the row index (left terms), the column index (right terms) or both
+// (jumps, sign taken over r and c).  Single-qubit diagonal jumps are summed
+// into tables over groups of three qubits (index (row bits << 3) | col bits).
+struct QTerm {
+  uint32_t fmask, cmask, cval, smask;
+  double2 coef;
+};
+constexpr int QMAX_TERMS = 192;
+constexpr int QMAX_GROUPS = 10;
+struct QubitProg {
+  int n;         // qubits
+  int nL, nR, nJ, nJx;  // nJx: multi-qubit diagonal jumps (generic loop)
+  int real;      // 1: left/right coefficients purely imaginary, jump ones real
+  int ngroups;
+  const double2 *dr, *dc;   // device, D each
+  const double2 *gtab;      // device, ngroups * 64
+};
+
 struct DeviceProgram {
   DevProg dev{};
   HostProg host;
+  bool has_qubit = false;
+  QubitProg qdev{};
+  std::vector<QTerm> qterms;  // nL | nR | nJ | nJx in that order
   std::vector<void *> allocations;
   void release();
 };
@@ -92,8 +117,12 @@ struct DeviceProgram {
 // mode 0 = density matrix (L on D^2), 1 = Schroedinger (-iH on D).
 DeviceProgram *compile_terms(qsystem qs, int mode);
 
-// Kernel launchers (lrho.cu)
+// Kernel launchers (lrho.cu, lrho_qubit.cu)
 void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t s);
+void launch_lrho_qubit(const DeviceProgram &P, const double2 *x, const Epi &e, cudaStream_t s);
+// Dispatch: the qubit kernel when the program has one, else the generic one.
+void launch_lrho_any(const DeviceProgram &P, const double2 *x, const Epi &e, cudaStream_t s);
+bool compile_qubit(qsystem qs, const HostProg &hp, DeviceProgram *P);
 void zero_epi(Epi &e);
 
 }  // namespace quac

@@ -49,7 +49,7 @@ std::vector<Event> collect_events(qsystem qs, double t0, double tmax) {
 // Stage helpers -------------------------------------------------------
 struct Stepper {
   qsystem qs;
-  const DevProg *P;
+  const DeviceProgram *P;
   cudaStream_t s;
   int64_t n;
   double atol, rtol;
@@ -73,7 +73,7 @@ struct Stepper {
     e.nyn = nyn;
     e.atol = atol;
     e.rtol = rtol;
-    launch_lrho(*P, X, e, s);
+    launch_lrho_any(*P, X, e, s);
   }
 };
 
@@ -84,7 +84,8 @@ struct Stepper {
 int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int64_t steps_max) {
   ensure_program(qs);
   if (has_error() || !qs->impl->prog) return 1;
-  const DevProg &P = qs->impl->prog->dev;
+  const DeviceProgram &PP = *qs->impl->prog;
+  const DevProg &P = PP.dev;
   const int64_t n = v->n;
   if (n != (int64_t)P.D * P.ncols) {
     fail(0, "ERROR! qvec size %ld does not match the system dimension %ld\n", (long)n,
@@ -101,7 +102,7 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
   vec_sync_to_device(v);
   QCUDA(cudaDeviceSynchronize());
 
-  Stepper st{qs, &P, s, n, o.atol, o.rtol};
+  Stepper st{qs, &PP, s, n, o.atol, o.rtol};
   std::vector<Event> events = x ? collect_events(qs, t0, tmax) : std::vector<Event>();
   size_t next_ev = 0;
   _p_TS ts;
@@ -221,7 +222,7 @@ int quac_lrho_apply_device(qsystem qs, const void *x_dev, void *y_dev) {
   zero_epi(e);
   e.kout = (double2 *)y_dev;
   cudaStream_t s = stream_of(qs);
-  launch_lrho(qs->impl->prog->dev, (const double2 *)x_dev, e, s);
+  launch_lrho_any(*qs->impl->prog, (const double2 *)x_dev, e, s);
   QCUDA(cudaStreamSynchronize(s));
   return has_error() ? 1 : 0;
 }
@@ -237,7 +238,7 @@ int quac_lrho_apply_host(qsystem qs, const PetscScalar *x_host, PetscScalar *y_h
   Epi e;
   zero_epi(e);
   e.kout = W.bufs[1];
-  launch_lrho(qs->impl->prog->dev, W.bufs[0], e, s);
+  launch_lrho_any(*qs->impl->prog, W.bufs[0], e, s);
   QCUDA(cudaMemcpyAsync(y_host, W.bufs[1], n * sizeof(double2), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));
   return has_error() ? 1 : 0;

@@ -180,12 +180,12 @@ static Gmres &gmres_for(qsystem) {
 }
 
 // A x with A = L + e0 vec(I)^T
-static void apply_A(const DevProg &P, const double2 *x, double2 *y, cudaStream_t s) {
+static void apply_A(const DeviceProgram &PP, const double2 *x, double2 *y, cudaStream_t s) {
   Epi e;
   zero_epi(e);
   e.kout = y;
-  launch_lrho(P, x, e, s);
-  k_trace_add<<<1, NT, 0, s>>>(x, y, P.D);
+  launch_lrho_any(PP, x, e, s);
+  k_trace_add<<<1, NT, 0, s>>>(x, y, PP.dev.D);
   count_launch();
 }
 
@@ -197,7 +197,8 @@ static double norm2(const double2 *x, int64_t n, cudaStream_t s) {
 int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, bool x_is_guess,
                     double *final_res) {
   ensure_program(qs);
-  const DevProg &P = qs->impl->prog->dev;
+  const DeviceProgram &PP = *qs->impl->prog;
+  const DevProg &P = PP.dev;
   const int64_t n = (int64_t)P.D * P.ncols;
   cudaStream_t s = stream_of(qs);
   if (m < 1 || m > 127) { fail(9, "ERROR! GMRES restart must be in [1, 127]\n"); return -1; }
@@ -213,7 +214,7 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
   double res = 0;
   while (true) {
     // r = b - A x  -> V_0
-    apply_A(P, x, G.V, s);
+    apply_A(PP, x, G.V, s);
     k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.V, n);
     count_launch();
     const double beta = norm2(G.V, n, s);
@@ -226,7 +227,7 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
     int j = 0;
     bool conv = false;
     for (; j < m && it < maxit; j++, it++) {
-      apply_A(P, G.V + (size_t)j * n, G.w, s);
+      apply_A(PP, G.V + (size_t)j * n, G.w, s);
       // CGS2 with the projections summed on the host
       std::vector<std::complex<double>> hsum(j + 1, 0.0);
       for (int pass = 0; pass < 2; pass++) {

@@ -256,6 +256,8 @@ DeviceProgram *compile_terms(qsystem qs, int mode) {
   d.dr = upload(P, to_d2(hp.dr));
   d.dc = upload(P, to_d2(hp.dc));
   d.qubit_path = 0;
+  if (options().kernel_path == 0 && mode == 0) compile_qubit(qs, hp, P);
+  d.qubit_path = P->has_qubit ? 1 : 0;
   return P;
 }
 

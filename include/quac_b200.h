@@ -272,9 +272,11 @@ void *quac_qvec_device_ptr(qvec q);
 /* Launch this system's kernels on a caller-owned CUDA stream (NULL: the
  * library's own stream). */
 void quac_set_stream(qsystem qsys, void *cuda_stream);
-/* Kernel selection for systems compiled afterwards: 0 = bit-mask kernel for
- * all-qubit systems of six or more qubits (default), 1 = generic table
- * kernel for every system. */
+/* Kernel selection for systems compiled afterwards: 0 = default (multi-pass
+ * bit-mask kernel for all-qubit systems of seven or more qubits, single-pass
+ * bit-mask kernel for six, generic table kernel otherwise), 1 = generic
+ * table kernel for every system, 2 = single-pass bit-mask kernel whenever
+ * the system is all-qubit. */
 void quac_set_kernel_path(int path);
 /* Number of kernels this library has launched (diagnostics). */
 int64_t quac_kernel_launch_count(void);

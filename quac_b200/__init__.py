@@ -628,5 +628,5 @@ def set_stream(qs, stream_ptr):
 
 
 def set_kernel_path(path):
-    """0: bit-mask kernel for all-qubit systems (default); 1: generic kernel only."""
+    """0: default selection; 1: generic table kernel; 2: single-pass bit-mask kernel."""
     lib().quac_set_kernel_path(int(path))

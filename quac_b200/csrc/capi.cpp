@@ -186,6 +186,7 @@ void QuaC_initialize(int argc, char **args) {
     const char *a = args[i];
     const char *v = (i + 1 < argc) ? args[i + 1] : "";
     if (!strcmp(a, "-ts_rk_type")) { o.rk_type = v; i++; }
+    else if (!strcmp(a, "-quac_rk4_classic")) { o.rk4_classic = true; }
     else if (!strcmp(a, "-ts_adapt_type")) { o.adapt_type = v; i++; }
     else if (!strcmp(a, "-ts_rtol")) { o.rtol = atof(v); o.rtol_set = true; i++; }
     else if (!strcmp(a, "-ts_atol")) { o.atol = atof(v); o.atol_set = true; i++; }
@@ -215,8 +216,9 @@ int quac_set_ts_options(const char *rk_type, const char *adapt_type, double rtol
   Options &o = options();
   if (rk_type && *rk_type) {
     std::string s(rk_type);
-    if (s != "3bs" && s != "4" && s != "5dp") { fail(9, "ERROR! unknown rk type %s\n", rk_type); return 1; }
-    o.rk_type = s;
+    if (s != "3bs" && s != "4" && s != "5dp" && s != "4classic") { fail(9, "ERROR! unknown rk type %s\n", rk_type); return 1; }
+    o.rk4_classic = (s == "4classic");
+    o.rk_type = (s == "4classic") ? "4" : s;
   }
   if (adapt_type && *adapt_type) {
     std::string s(adapt_type);

@@ -103,10 +103,34 @@ struct QubitProg {
   const double2 *gtab;      // device, ngroups * 64
 };
 
+// One pass of the multi-pass qubit kernel (lrho_q2.cu).
+constexpr int MAXPT = 128;  // terms per pass
+struct PassTerm {
+  uint32_t fl;  // flip mask in tile coordinates (cross-group terms: full mask | kind << 29)
+  uint32_t cmask, cval, smask;
+  double2 coef;
+};
+struct PassParams {
+  int n, lo;             // qubits, first bit of this pass's six-bit group
+  int nL, nR, nJ, nJx;
+  int first, last;
+  int real;
+  int ngroups;
+  int nspill;            // cross-group terms handled with global loads (last pass)
+  long long ntiles;
+  const double2 *dr, *dc, *gtab;
+  const double2 *accin;  // running sum from earlier passes
+  double2 *accout;       // running sum for later passes
+  int *errflag;
+  PassTerm t[MAXPT];
+};
+
 struct DeviceProgram {
   DevProg dev{};
   HostProg host;
   bool has_qubit = false;
+  std::vector<PassParams> passes;  // non-empty: multi-pass qubit kernel
+  double2 *scratch = nullptr;      // D^2 running sum for the passes
   QubitProg qdev{};
   std::vector<QTerm> qterms;  // nL | nR | nJ | nJx in that order
   std::vector<void *> allocations;
@@ -123,6 +147,9 @@ void launch_lrho_qubit(const DeviceProgram &P, const double2 *x, const Epi &e, c
 // Dispatch: the qubit kernel when the program has one, else the generic one.
 void launch_lrho_any(const DeviceProgram &P, const double2 *x, const Epi &e, cudaStream_t s);
 bool compile_qubit(qsystem qs, const HostProg &hp, DeviceProgram *P);
+bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out);
+void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
+                         const Epi &e, cudaStream_t s);
 void zero_epi(Epi &e);
 
 }  // namespace quac

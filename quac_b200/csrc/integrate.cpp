@@ -129,7 +129,17 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
     double2 *y = v->d;
     bool accepted = true;
     double h_next = h;
-    if (fixed && rk4) {
+    if (fixed && rk4 && !o.rk4_classic) {
+      // For a time-independent linear right-hand side the classical RK4 step
+      // equals the degree-4 Taylor polynomial of exp(hL); evaluated by
+      // Horner's rule each stage reads one vector besides its input:
+      //   v <- y + (h/4) L y;  v <- y + (h/3) L v;  v <- y + (h/2) L v;  y <- y + h L v
+      double2 *va = W.bufs[0], *vb = W.bufs[1];
+      st.stage(y, {{va, y, h_try / 4.0}});
+      st.stage(va, {{vb, y, h_try / 3.0}});
+      st.stage(vb, {{va, y, h_try / 2.0}});
+      st.stage(va, {{y, y, h_try}});
+    } else if (fixed && rk4) {
       double2 *acc = W.bufs[0], *xa = W.bufs[1], *xb = W.bufs[2];
       st.stage(y, {{acc, y, h_try / 6.0}, {xa, y, h_try / 2.0}});
       st.stage(xa, {{acc, acc, h_try / 3.0}, {xb, y, h_try / 2.0}});

@@ -262,8 +262,19 @@ void launch_lrho_qubit(const DeviceProgram &P, const double2 *x, const Epi &e, c
 }
 
 void launch_lrho_any(const DeviceProgram &P, const double2 *x, const Epi &e, cudaStream_t s) {
-  if (P.has_qubit) launch_lrho_qubit(P, x, e, s);
-  else launch_lrho(P.dev, x, e, s);
+  if (P.has_qubit && !P.passes.empty()) {
+    DeviceProgram &M = const_cast<DeviceProgram &>(P);
+    if (!M.scratch) {
+      const size_t n = (size_t)P.dev.D * P.dev.ncols;
+      QCUDA(cudaMalloc(&M.scratch, n * sizeof(double2)));
+      M.allocations.push_back(M.scratch);
+    }
+    launch_qubit_passes(M.passes, x, M.scratch, e, s);
+  } else if (P.has_qubit) {
+    launch_lrho_qubit(P, x, e, s);
+  } else {
+    launch_lrho(P.dev, x, e, s);
+  }
 }
 
 }  // namespace quac

@@ -35,7 +35,8 @@ struct Options {
   double rtol = 5e-7, atol = 5e-7;  // qsystem.c:902
   int64_t max_steps = -1;           // -1: use the caller's steps_max
   bool rtol_set = false, atol_set = false;
-  int kernel_path = 0;              // 0: qubit kernel when applicable, 1: generic only
+  int kernel_path = 0;              // see quac_set_kernel_path
+  bool rk4_classic = false;         // rk_type "4classic": four-stage form instead of Horner
 };
 Options &options();
 

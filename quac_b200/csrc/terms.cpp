@@ -102,6 +102,7 @@ void op_chain_map(int64_t D, const std::vector<op_handle> &ops, std::vector<int>
 void DeviceProgram::release() {
   for (void *p : allocations) cudaFree(p);
   allocations.clear();
+  scratch = nullptr;
 }
 
 namespace {
@@ -256,7 +257,10 @@ DeviceProgram *compile_terms(qsystem qs, int mode) {
   d.dr = upload(P, to_d2(hp.dr));
   d.dc = upload(P, to_d2(hp.dc));
   d.qubit_path = 0;
-  if (options().kernel_path == 0 && mode == 0) compile_qubit(qs, hp, P);
+  if (options().kernel_path != 1 && mode == 0) compile_qubit(qs, hp, P);
+  if (P->has_qubit && options().kernel_path != 2) {
+    if (!plan_qubit_passes(*P, P->passes)) P->passes.clear();
+  }
   d.qubit_path = P->has_qubit ? 1 : 0;
   return P;
 }

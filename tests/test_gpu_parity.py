@@ -311,6 +311,8 @@ def qubit_zoo(S, n=7):
     S.lin(0.04, qs[1].n, qs[5].n)
     S.lin(0.01 + 0.002j, qs[n - 3].dag)
     S.lin(0.06, qs[2].sig_x)
+    S.ham(0.12, qs[0].sig_x, qs[n - 1].sig_x)   # flips in two bit groups
+    S.lin(0.015, qs[n - 1].a, qs[0].dag)
     return qs
 
 
@@ -334,18 +336,20 @@ def test_qubit_kernel_matches_oracle(quac, oracle, n, build):
     S.qs.destroy()
 
 
-def test_qubit_and_generic_kernels_agree(quac):
+@pytest.mark.parametrize("n", [8, 11])
+def test_qubit_and_generic_kernels_agree(quac, n):
     ys = []
-    for path in (0, 1):
+    for path in (0, 1, 2):
         quac.set_kernel_path(path)
         S = H.ProductSystem(quac)
-        qubit_zoo(S, 8)
+        qubit_zoo(S, n)
         quac.construct_matrix(S.qs)
         x = H.random_state(S.D, seed=9)
         ys.append(quac.lrho_apply_host(S.qs, x))
         S.qs.destroy()
     quac.set_kernel_path(0)
     assert _rel(ys[0], ys[1]) < 1e-13
+    assert _rel(ys[2], ys[1]) < 1e-13
 
 
 def test_full_size_tfim12_properties(quac, oracle):
@@ -374,4 +378,42 @@ def test_full_size_tfim12_properties(quac, oracle):
     y2 = quac.lrho_apply_host(S.qs, x2)
     y12 = quac.lrho_apply_host(S.qs, 0.3 * x + 2.0 * x2)
     assert _rel(y12, 0.3 * y + 2.0 * y2) < 1e-13
+    S.qs.destroy()
+
+
+def test_rk4_horner_equals_classical(quac):
+    outs = []
+    for form in ("4", "4classic"):
+        S = H.ProductSystem(quac)
+        H.tfim(S, 8)
+        quac.construct_matrix(S.qs)
+        rho = quac.create_dm_sys(S.qs)
+        rho.from_numpy(H.random_state(S.D, seed=4, hermitian=True))
+        quac.set_ts_options(rk_type=form, adapt_type="none")
+        quac.time_step_sys(S.qs, rho, 0.0, 1.0, 0.01, 10 ** 6)
+        outs.append(rho.to_numpy())
+        rho.destroy()
+        S.qs.destroy()
+    quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+    assert _rel(outs[0], outs[1]) < 1e-13
+
+
+def test_multipass_rk4_tfim9_matches_oracle(quac, oracle):
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.tfim(S, 9)
+    H.tfim(O, 9)
+    quac.construct_matrix(S.qs)
+    D = S.D
+    x0 = H.random_state(D, seed=6, hermitian=True)
+    rho = quac.create_dm_sys(S.qs)
+    rho.from_numpy(x0)
+    quac.set_ts_options(rk_type="4", adapt_type="none")
+    quac.time_step_sys(S.qs, rho, 0.0, 0.2, 0.01, 10 ** 6)
+    quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+    h = O.csr_handle()
+    yo = oracle.rk4(h, x0, 0.01, 20)
+    oracle.free_csr(h)
+    assert _rel(rho.to_numpy(), yo) < 1e-12
+    rho.destroy()
     S.qs.destroy()

@@ -112,16 +112,21 @@ struct PassTerm {
 };
 struct PassParams {
   int n, lo;             // qubits, first bit of this pass's six-bit group
-  int nL, nR, nJ, nJx;
-  int first, last;
+  int nL, nR, nJ, nJx;   // general terms
+  int diag;              // this pass applies the diagonal (dr, dc, group tables, nJx)
+  int last;              // this pass runs the stage epilogue
   int real;
   int ngroups;
   int nspill;            // cross-group terms handled with global loads (last pass)
+  int ncanon;            // nonzero: canonical single-bit coefficients below are used
   long long ntiles;
   const double2 *dr, *dc, *gtab;
-  const double2 *accin;  // running sum from earlier passes
+  const double2 *accin;  // running sum from earlier passes (nullptr: start from zero)
   double2 *accout;       // running sum for later passes
   int *errflag;
+  // canonical single-bit terms of this group (real mode): left X (i*hl),
+  // right X (i*hr), lowering jump (gl, both bits 0), raising jump (gu, both 1)
+  double hl[6], hr[6], gl[6], gu[6];
   PassTerm t[MAXPT];
 };
 

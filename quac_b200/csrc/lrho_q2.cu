@@ -15,6 +15,7 @@
 // whose tiles have single-element rows the two halves of every 32-byte
 // sector are requested by neighbouring CTAs at the same time.
 #include <algorithm>
+#include <array>
 #include <cstring>
 
 #include "common.h"
@@ -78,12 +79,15 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
                                                  const double2 *__restrict__ X, const Epi E) {
   extern __shared__ double2 sm[];
   double2 *buf0 = sm, *buf1 = sm + NEL;
-  double2 *gts = sm + 2 * NEL;                 // ngroups * 64 (pass 0)
+  double2 *gts = sm + 2 * NEL;                 // ngroups * 64, layout [g][col bits][row bits]
   __shared__ double red[PT / 32];
   const int n = P.n, lo = P.lo;
   const size_t D = (size_t)1 << n;
-  if (P.first)
-    for (int i = threadIdx.x; i < P.ngroups * 64; i += PT) gts[i] = P.gtab[i];
+  if (P.diag)
+    for (int i = threadIdx.x; i < P.ngroups * 64; i += PT) {
+      const int g = i >> 6, rb = (i >> 3) & 7, cb = i & 7;  // source layout [g][rb][cb]
+      gts[(g << 6) | (cb << 3) | rb] = P.gtab[i];
+    }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double nloc = 0.0;
   long long t = blockIdx.x;
@@ -108,28 +112,89 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
 #pragma unroll
     for (int m = 0; m < 4; m++) c[m] = cfix | (cl[m] << lo);
     double2 acc[2][4];
-    if (P.first) {
+    if (P.accin) {
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) acc[i][m] = P.accin[(size_t)c[m] * D + r[i]];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) acc[i][m] = make_double2(0.0, 0.0);
+    }
+    if (P.diag) {
+      // groups 0 and 1 vary inside the tile (lo == 0 here); the others are
+      // fixed by the tile origin
+      double2 gconst = make_double2(0.0, 0.0);
+      for (int g = 2; g < P.ngroups; g++) {
+        const double2 v = gts[(g << 6) | (((cfix >> (3 * g)) & 7u) << 3) | ((rfix >> (3 * g)) & 7u)];
+        gconst.x += v.x;
+        gconst.y += v.y;
+      }
 #pragma unroll
       for (int i = 0; i < 2; i++) {
-        const double2 dri = __ldg(P.dr + r[i]);
+        double2 dri = __ldg(P.dr + r[i]);
+        dri.x += gconst.x;
+        dri.y += gconst.y;
 #pragma unroll
         for (int m = 0; m < 4; m++) {
           double2 d = __ldg(P.dc + c[m]);
           d.x += dri.x;
           d.y += dri.y;
-          for (int g = 0; g < P.ngroups; g++) {
-            const double2 v = gts[g * 64 + (((r[i] >> (3 * g)) & 7u) << 3) + ((c[m] >> (3 * g)) & 7u)];
-            d.x += v.x;
-            d.y += v.y;
+          const double2 v0 = gts[((c[m] & 7u) << 3) | (r[i] & 7u)];
+          d.x += v0.x;
+          d.y += v0.y;
+          if (P.ngroups > 1) {
+            const double2 v1 = gts[64 | (((c[m] >> 3) & 7u) << 3) | ((r[i] >> 3) & 7u)];
+            d.x += v1.x;
+            d.y += v1.y;
           }
-          acc[i][m] = cmul2(d, cur[cl[m] * 64 + rl[i]]);
+          cfma2(acc[i][m], d, cur[cl[m] * 64 + rl[i]]);
         }
       }
-    } else {
+    }
+    if (REAL && P.ncanon) {
+      // canonical single-bit terms: partner offsets are compile-time constants
 #pragma unroll
-      for (int i = 0; i < 2; i++)
+      for (int b = 0; b < 6; b++) {
+        const unsigned f = 1u << b;
+        const double hl = P.hl[b], hr = P.hr[b], gl = P.gl[b], gu = P.gu[b];
+        if (hl != 0.0) {
 #pragma unroll
-        for (int m = 0; m < 4; m++) acc[i][m] = P.accin[(size_t)c[m] * D + r[i]];
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+              const double2 p = cur[cl[m] * 64 + (rl[i] ^ f)];
+              acc[i][m].x = fma(-hl, p.y, acc[i][m].x);
+              acc[i][m].y = fma(hl, p.x, acc[i][m].y);
+            }
+        }
+        if (hr != 0.0) {
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+              const double2 p = cur[(cl[m] ^ f) * 64 + rl[i]];
+              acc[i][m].x = fma(-hr, p.y, acc[i][m].x);
+              acc[i][m].y = fma(hr, p.x, acc[i][m].y);
+            }
+        }
+        if (gl != 0.0 || gu != 0.0) {
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+              const bool rb = rl[i] & f, cb = cl[m] & f;
+              if (rb == cb) {
+                const double g = rb ? gu : gl;
+                const double2 p = cur[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
+                acc[i][m].x = fma(g, p.x, acc[i][m].x);
+                acc[i][m].y = fma(g, p.y, acc[i][m].y);
+              }
+            }
+        }
+      }
     }
     int k = 0;
     for (int e = k + P.nL; k < e; k++) {
@@ -198,7 +263,7 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         }
       }
     }
-    for (int e = k + P.nJx; k < e; k++) {  // multi-qubit diagonal jumps (pass 0)
+    for (int e = k + P.nJx; k < e; k++) {  // multi-qubit diagonal jumps (diagonal pass)
       const PassTerm T = P.t[k];
 #pragma unroll
       for (int i = 0; i < 2; i++) {
@@ -313,14 +378,16 @@ bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out) {
   const QubitProg &Q = P.qdev;
   const int n = Q.n;
   if (n < 7 || n > 16) return false;
+  // groups of six bit positions; the last may overlap its neighbour
   std::vector<int> los;
   for (int lo = 0; lo < n; lo += 6) los.push_back(std::min(lo, n - 6));
-  const int np = (int)los.size();
-  out.assign(np, PassParams());
-  std::vector<std::vector<PassTerm>> L(np), R(np), J(np);
+  const int ng = (int)los.size();
+  std::vector<std::vector<PassTerm>> L(ng), R(ng), J(ng);
   std::vector<PassTerm> Jx, spill;
+  std::vector<std::array<double, 24>> canon(ng);
+  for (auto &cv : canon) cv.fill(0.0);
   auto group_of = [&](uint32_t f) -> int {
-    for (int p = 0; p < np; p++) {
+    for (int p = 0; p < ng; p++) {
       const uint32_t gm = 0x3fu << los[p];
       if ((f & ~gm) == 0) return p;
     }
@@ -335,6 +402,7 @@ bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out) {
     t.coef = q.coef;
     return t;
   };
+  const bool real = Q.real != 0;
   const auto &qt = P.qterms;
   size_t k = 0;
   for (int kind = 0; kind < 4; kind++) {
@@ -347,24 +415,46 @@ bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out) {
         spill.push_back(mk(q, q.fmask | ((uint32_t)kind << 29)));
         continue;
       }
-      PassTerm t = mk(q, q.fmask >> los[p]);
-      (kind == 0 ? L : kind == 1 ? R : J)[p].push_back(t);
+      const uint32_t fl = q.fmask >> los[p];
+      if (real && __builtin_popcount(fl) == 1) {
+        int b = 0;
+        while ((1u << b) != fl) b++;
+        if (kind < 2 && q.cmask == 0 && q.smask == 0) {
+          canon[p][kind * 6 + b] += q.coef.y;
+          continue;
+        }
+        if (kind == 2 && q.cmask == q.fmask && q.smask == 0) {
+          canon[p][(q.cval ? 18 : 12) + b] += q.coef.x;
+          continue;
+        }
+      }
+      (kind == 0 ? L : kind == 1 ? R : J)[p].push_back(mk(q, fl));
     }
   }
+  // pass order: the high groups first, group 0 (contiguous rows, diagonal,
+  // stage epilogue) last
   const long long ntiles = 1ll << (2 * n - 12);
-  for (int p = 0; p < np; p++) {
-    PassParams &pp = out[p];
+  out.clear();
+  for (int p = ng - 1; p >= 0; p--) {
+    PassParams pp;
     memset(&pp, 0, sizeof(pp));
     pp.n = n;
     pp.lo = los[p];
-    pp.first = p == 0;
-    pp.last = p == np - 1;
+    pp.diag = p == 0;
+    pp.last = p == 0;
     pp.real = Q.real;
     pp.ngroups = Q.ngroups;
     pp.ntiles = ntiles;
     pp.dr = Q.dr;
     pp.dc = Q.dc;
     pp.gtab = Q.gtab;
+    for (int b = 0; b < 6; b++) {
+      pp.hl[b] = canon[p][b];
+      pp.hr[b] = canon[p][6 + b];
+      pp.gl[b] = canon[p][12 + b];
+      pp.gu[b] = canon[p][18 + b];
+      if (pp.hl[b] != 0 || pp.hr[b] != 0 || pp.gl[b] != 0 || pp.gu[b] != 0) pp.ncanon = 1;
+    }
     std::vector<PassTerm> all;
     all.insert(all.end(), L[p].begin(), L[p].end());
     all.insert(all.end(), R[p].begin(), R[p].end());
@@ -375,13 +465,12 @@ bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out) {
     if (p == 0) {
       all.insert(all.end(), Jx.begin(), Jx.end());
       pp.nJx = (int)Jx.size();
-    }
-    if (pp.last) {
       all.insert(all.end(), spill.begin(), spill.end());
       pp.nspill = (int)spill.size();
     }
     if (all.size() > (size_t)MAXPT) return false;
     for (size_t i = 0; i < all.size(); i++) pp.t[i] = all[i];
+    out.push_back(pp);
   }
   return true;
 }

@@ -320,9 +320,22 @@ def tfim_real(S, n):
     return H.tfim(S, n)
 
 
+def tfim_pump(S, n):
+    """Real-coefficient system that exercises every canonical single-bit
+    slot (X fields, decay, pumping) plus general and cross-group terms."""
+    qs = H.tfim(S, n)
+    for q in qs[::3]:
+        S.lin(2e-3, q.dag)
+    S.ham(0.11, qs[0].sig_x, qs[n - 1].sig_x)
+    S.ham(0.07, qs[1].sig_x, qs[2].sig_x)
+    S.lin(0.01, qs[n - 2].a, qs[0].a)
+    return qs
+
+
 @pytest.mark.parametrize("n,build", [(6, qubit_zoo), (7, qubit_zoo), (9, qubit_zoo),
-                                     (6, tfim_real), (10, tfim_real)],
-                         ids=["zoo6", "zoo7", "zoo9", "tfim6", "tfim10"])
+                                     (6, tfim_real), (10, tfim_real), (7, tfim_pump),
+                                     (11, tfim_pump)],
+                         ids=["zoo6", "zoo7", "zoo9", "tfim6", "tfim10", "pump7", "pump11"])
 def test_qubit_kernel_matches_oracle(quac, oracle, n, build):
     S = H.ProductSystem(quac)
     O = oracle.OSys()

@@ -124,6 +124,11 @@ struct PassParams {
   const double2 *accin;  // running sum from earlier passes (nullptr: start from zero)
   double2 *accout;       // running sum for later passes
   int *errflag;
+  // TMA view of the tile (used when tma != 0): dims 1..4 of the 5-D tensor
+  // map start at flat index bit tstart[d] with tlen[d] bits; tfree[d] marks
+  // the dims the box covers fully (their coordinate is 0)
+  int tma;
+  int tstart[5], tlen[5], tfree[5];
   // canonical single-bit terms of this group (real mode): left X (i*hl),
   // right X (i*hr), lowering jump (gl, both bits 0), raising jump (gu, both 1)
   double hl[6], hr[6], gl[6], gu[6];
@@ -136,6 +141,7 @@ struct DeviceProgram {
   bool has_qubit = false;
   std::vector<PassParams> passes;  // non-empty: multi-pass qubit kernel
   double2 *scratch = nullptr;      // D^2 running sum for the passes
+  int *errflag = nullptr;          // device word set by kernels whose waits time out
   QubitProg qdev{};
   std::vector<QTerm> qterms;  // nL | nR | nJ | nJx in that order
   std::vector<void *> allocations;
@@ -155,6 +161,8 @@ bool compile_qubit(qsystem qs, const HostProg &hp, DeviceProgram *P);
 bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out);
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
                          const Epi &e, cudaStream_t s);
+// Reads and clears the program's device error word; reports through fail().
+bool check_program_error(DeviceProgram &P, cudaStream_t s);
 void zero_epi(Epi &e);
 
 }  // namespace quac

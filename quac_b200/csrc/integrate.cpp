@@ -197,6 +197,7 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
     }
   }
   QCUDA(cudaStreamSynchronize(s));
+  check_program_error(*qs->impl->prog, s);
   qs->current_time = t;
   if (std::fabs(t - tmax) > 1e-8 && !has_error()) printf("ERROR! Did not reach final time! Reason: %d\n", -1);
   return has_error() ? 1 : 0;
@@ -234,6 +235,7 @@ int quac_lrho_apply_device(qsystem qs, const void *x_dev, void *y_dev) {
   cudaStream_t s = stream_of(qs);
   launch_lrho_any(*qs->impl->prog, (const double2 *)x_dev, e, s);
   QCUDA(cudaStreamSynchronize(s));
+  check_program_error(*qs->impl->prog, s);
   return has_error() ? 1 : 0;
 }
 
@@ -251,6 +253,7 @@ int quac_lrho_apply_host(qsystem qs, const PetscScalar *x_host, PetscScalar *y_h
   launch_lrho_any(*qs->impl->prog, W.bufs[0], e, s);
   QCUDA(cudaMemcpyAsync(y_host, W.bufs[1], n * sizeof(double2), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));
+  check_program_error(*qs->impl->prog, s);
   return has_error() ? 1 : 0;
 }
 

@@ -18,6 +18,8 @@
 #include <array>
 #include <cstring>
 
+#include <cuda.h>
+
 #include "common.h"
 
 namespace quac {
@@ -45,6 +47,42 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int c0, int c1, int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+      "r"(smem_u32(bar))
+      : "memory");
+}
 
 // fixed (non-tile) bits of a work item: rows then columns
 __device__ __forceinline__ void tile_origin(long long t, int n, int lo, unsigned &rfix, unsigned &cfix) {
@@ -74,13 +112,29 @@ __device__ __forceinline__ void load_tile(double2 *buf, const double2 *__restric
   }
 }
 
-template <bool REAL>
+// issues the TMA load of work item t into buf (thread 0 only)
+__device__ __forceinline__ void tma_tile(const PassParams &P, const CUtensorMap *map, double2 *buf,
+                                         uint64_t *bar, long long t) {
+  unsigned rfix, cfix;
+  tile_origin(t, P.n, P.lo, rfix, cfix);
+  const unsigned long long F = (unsigned long long)rfix | ((unsigned long long)cfix << P.n);
+  int c[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+  for (int d = 1; d < 5; d++)
+    c[d] = P.tfree[d] ? 0 : (int)((F >> P.tstart[d]) & ((1ull << P.tlen[d]) - 1ull));
+  mbar_expect_tx(bar, NEL * sizeof(double2));
+  tma_load_5d(buf, map, bar, c[0], c[1], c[2], c[3], c[4]);
+}
+
+template <bool REAL, bool TMA>
 __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassParams P,
+                                                 const __grid_constant__ CUtensorMap tmap,
                                                  const double2 *__restrict__ X, const Epi E) {
-  extern __shared__ double2 sm[];
-  double2 *buf0 = sm, *buf1 = sm + NEL;
-  double2 *gts = sm + 2 * NEL;                 // ngroups * 64, layout [g][col bits][row bits]
+  constexpr int NST = TMA ? 3 : 2;   // pipeline stages
+  extern __shared__ __align__(128) double2 sm[];
+  double2 *gts = sm + NST * NEL;     // ngroups * 64, layout [g][col bits][row bits]
   __shared__ double red[PT / 32];
+  __shared__ __align__(8) uint64_t bars[3];
   const int n = P.n, lo = P.lo;
   const size_t D = (size_t)1 << n;
   if (P.diag)
@@ -90,17 +144,46 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
     }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double nloc = 0.0;
-  long long t = blockIdx.x;
-  if (t < P.ntiles) load_tile(buf0, X, t, n, lo);
-  cp_commit();
-  for (int it = 0; t < P.ntiles; it++, t += gridDim.x) {
-    const long long tn = t + gridDim.x;
-    double2 *cur = (it & 1) ? buf1 : buf0;
-    double2 *nxt = (it & 1) ? buf0 : buf1;
-    if (tn < P.ntiles) load_tile(nxt, X, tn, n, lo);
-    cp_commit();
-    cp_wait<1>();
+  if (TMA) {
+    if (threadIdx.x == 0) {
+      for (int q = 0; q < 3; q++) mbar_init(&bars[q], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
     __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int q = 0; q < 2; q++) {
+        const long long tq = blockIdx.x + (long long)q * gridDim.x;
+        if (tq < P.ntiles) tma_tile(P, &tmap, sm + q * NEL, &bars[q], tq);
+      }
+    }
+  } else {
+    if (blockIdx.x < P.ntiles) load_tile(sm, X, blockIdx.x, n, lo);
+    cp_commit();
+  }
+  long long t = blockIdx.x;
+  for (int it = 0; t < P.ntiles; it++, t += gridDim.x) {
+    double2 *cur = sm + (it % NST) * NEL;
+    if (TMA) {
+      const long long t2 = t + 2ll * gridDim.x;
+      if (threadIdx.x == 0 && t2 < P.ntiles)
+        tma_tile(P, &tmap, sm + ((it + 2) % 3) * NEL, &bars[(it + 2) % 3], t2);
+      const unsigned parity = (unsigned)((it / 3) & 1);
+      const unsigned long long t0 = global_ns();
+      bool timed_out = false;
+      while (!mbar_try_wait(&bars[it % 3], parity)) {
+        if (global_ns() - t0 > 2000000000ull) { timed_out = true; break; }
+      }
+      if (__syncthreads_or(timed_out)) {
+        if (threadIdx.x == 0 && P.errflag) atomicExch(P.errflag, 1);
+        return;
+      }
+    } else {
+      const long long tn = t + gridDim.x;
+      if (tn < P.ntiles) load_tile(sm + ((it + 1) & 1) * NEL, X, tn, n, lo);
+      cp_commit();
+      cp_wait<1>();
+      __syncthreads();
+    }
     unsigned rfix, cfix;
     tile_origin(t, n, lo, rfix, cfix);
     // thread elements: rows lane, lane+32; columns w, w+16, w+32, w+48
@@ -345,9 +428,9 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         }
       }
     }
-    __syncthreads();  // cur is refilled two iterations later
+    __syncthreads();  // every thread is done with cur before it is refilled
   }
-  cp_wait<0>();
+  if (!TMA) cp_wait<0>();
   if (P.last && E.nsum) {
     for (int o = 16; o > 0; o >>= 1) nloc += __shfl_down_sync(0xffffffffu, nloc, o);
     if (lane == 0) red[w] = nloc;
@@ -368,6 +451,91 @@ int num_sms() {
     QCUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
   }
   return n;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                    const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                    const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    QCUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) fail(9, "ERROR! cuTensorMapEncodeTiled unavailable\n");
+    fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// Describes the 64x64 tile of a pass as a 5-D box over the flat index.
+// Returns false when the runs of fixed and free bits need more than five
+// dimensions (then the cp.async path is used).
+bool describe_tma(PassParams &pp) {
+  const int n = pp.n, lo = pp.lo;
+  struct Run { int start, len; bool free; };
+  std::vector<Run> runs;
+  auto add = [&](int start, int len, bool fr) {
+    if (len <= 0) return;
+    if (!runs.empty() && runs.back().free == fr && runs.back().start + runs.back().len == start)
+      runs.back().len += len;
+    else
+      runs.push_back({start, len, fr});
+  };
+  add(0, lo, false);
+  add(lo, 6, true);
+  add(lo + 6, n - lo - 6, false);
+  add(n, lo, false);
+  add(n + lo, 6, true);
+  add(n + lo + 6, n - lo - 6, false);
+  // dim 0 = the element (two doubles), merged with a leading free run
+  int first = 0;
+  if (!runs.empty() && runs[0].start == 0 && runs[0].free) first = 1;
+  const int ndims = 1 + (int)runs.size() - first;
+  if (ndims > 5) return false;
+  pp.tstart[0] = 0;
+  pp.tlen[0] = first ? runs[0].len : 0;
+  pp.tfree[0] = 1;
+  int d = 1;
+  for (size_t k = first; k < runs.size(); k++, d++) {
+    pp.tstart[d] = runs[k].start;
+    pp.tlen[d] = runs[k].len;
+    pp.tfree[d] = runs[k].free ? 1 : 0;
+  }
+  for (; d < 5; d++) {  // padding dims of size one
+    pp.tstart[d] = 2 * n;
+    pp.tlen[d] = 0;
+    pp.tfree[d] = 1;
+  }
+  return true;
+}
+
+void encode_tma(const PassParams &pp, const double2 *x, CUtensorMap *map) {
+  cuuint64_t dims[5], strides[4];
+  cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+  dims[0] = 2ull << pp.tlen[0];
+  box[0] = 2u << pp.tlen[0];
+  for (int d = 1; d < 5; d++) {
+    dims[d] = 1ull << pp.tlen[d];
+    box[d] = pp.tfree[d] ? (1u << pp.tlen[d]) : 1u;
+    strides[d - 1] = 16ull << pp.tstart[d];
+  }
+  CUresult r = encode_fn()(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, (void *)x, dims, strides, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(9, "ERROR! cuTensorMapEncodeTiled failed (%d)\n", (int)r);
+}
+
+template <bool REAL, bool TMA>
+void set_smem_attr(size_t smem) {
+  static bool done = false;
+  if (!done) {
+    QCUDA(cudaFuncSetAttribute(k_qpass<REAL, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
+    done = true;
+  }
 }
 
 }  // namespace
@@ -470,7 +638,22 @@ bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out) {
     }
     if (all.size() > (size_t)MAXPT) return false;
     for (size_t i = 0; i < all.size(); i++) pp.t[i] = all[i];
+    pp.tma = describe_tma(pp) ? 1 : 0;
+    pp.errflag = P.errflag;
     out.push_back(pp);
+  }
+  return true;
+}
+
+bool check_program_error(DeviceProgram &P, cudaStream_t s) {
+  if (!P.errflag) return true;
+  int h = 0;
+  QCUDA(cudaMemcpyAsync(&h, P.errflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  QCUDA(cudaStreamSynchronize(s));
+  if (h) {
+    QCUDA(cudaMemsetAsync(P.errflag, 0, sizeof(int), s));
+    fail(9, "ERROR! a tile load did not complete within its time limit; results are invalid\n");
+    return false;
   }
   return true;
 }
@@ -480,21 +663,21 @@ bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out) {
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
                          const Epi &e, cudaStream_t s) {
   const int np = (int)passes.size();
-  const size_t smem = (size_t)(2 * NEL + QMAX_GROUPS * 64) * sizeof(double2);
-  static bool attr = false;
-  if (!attr) {
-    QCUDA(cudaFuncSetAttribute(k_qpass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    QCUDA(cudaFuncSetAttribute(k_qpass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
   const long long nt = passes[0].ntiles;
   const int grid = (int)std::min<long long>(nt, num_sms());
   for (int p = 0; p < np; p++) {
     PassParams &pp = passes[p];
     pp.accin = p > 0 ? scratch : nullptr;
     pp.accout = (p < np - 1) ? scratch : nullptr;
-    if (pp.real) k_qpass<true><<<grid, PT, smem, s>>>(pp, x, e);
-    else k_qpass<false><<<grid, PT, smem, s>>>(pp, x, e);
+    CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    const bool tma = pp.tma != 0;
+    if (tma) encode_tma(pp, x, &map);
+    const size_t smem = (size_t)((tma ? 3 : 2) * NEL + QMAX_GROUPS * 64) * sizeof(double2);
+    if (pp.real && tma) { set_smem_attr<true, true>(smem); k_qpass<true, true><<<grid, PT, smem, s>>>(pp, map, x, e); }
+    else if (pp.real) { set_smem_attr<true, false>(smem); k_qpass<true, false><<<grid, PT, smem, s>>>(pp, map, x, e); }
+    else if (tma) { set_smem_attr<false, true>(smem); k_qpass<false, true><<<grid, PT, smem, s>>>(pp, map, x, e); }
+    else { set_smem_attr<false, false>(smem); k_qpass<false, false><<<grid, PT, smem, s>>>(pp, map, x, e); }
     count_launch();
     QCUDA(cudaGetLastError());
   }

@@ -103,6 +103,7 @@ void DeviceProgram::release() {
   for (void *p : allocations) cudaFree(p);
   allocations.clear();
   scratch = nullptr;
+  errflag = nullptr;
 }
 
 namespace {
@@ -259,6 +260,9 @@ DeviceProgram *compile_terms(qsystem qs, int mode) {
   d.qubit_path = 0;
   if (options().kernel_path != 1 && mode == 0) compile_qubit(qs, hp, P);
   if (P->has_qubit && options().kernel_path != 2) {
+    QCUDA(cudaMalloc(&P->errflag, sizeof(int)));
+    QCUDA(cudaMemset(P->errflag, 0, sizeof(int)));
+    P->allocations.push_back(P->errflag);
     if (!plan_qubit_passes(*P, P->passes)) P->passes.clear();
   }
   d.qubit_path = P->has_qubit ? 1 : 0;

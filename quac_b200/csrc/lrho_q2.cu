@@ -26,7 +26,6 @@ namespace quac {
 
 namespace {
 
-constexpr int PT = 512;            // threads per CTA (16 warps)
 constexpr int TILE = 64;           // tile rows = tile columns
 constexpr int NEL = TILE * TILE;   // elements per tile
 __device__ __forceinline__ void cfma2(double2 &acc, double2 a, double2 b) {
@@ -105,7 +104,7 @@ __device__ __forceinline__ void load_tile(double2 *buf, const double2 *__restric
   unsigned rfix, cfix;
   tile_origin(t, n, lo, rfix, cfix);
   const size_t D = (size_t)1 << n;
-  for (int e = threadIdx.x; e < NEL; e += PT) {
+  for (int e = threadIdx.x; e < NEL; e += blockDim.x) {
     const unsigned cl = e >> 6, rl = e & 63;
     const size_t r = rfix | (rl << lo), c = cfix | (cl << lo);
     cp_async16(buf + e, X + c * D + r);
@@ -126,10 +125,18 @@ __device__ __forceinline__ void tma_tile(const PassParams &P, const CUtensorMap 
   tma_load_5d(buf, map, bar, c[0], c[1], c[2], c[3], c[4]);
 }
 
-template <bool REAL, bool TMA>
-__global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassParams P,
-                                                 const __grid_constant__ CUtensorMap tmap,
-                                                 const double2 *__restrict__ X, const Epi E) {
+// NTHR threads per CTA; each thread owns rows lane, lane+32 and MC columns
+// w, w + NW, ... (NW = NTHR / 32 warps).  CANON (real mode only) is a
+// compile-time mask of the canonical single-bit kinds present: 1 = left X,
+// 2 = right X, 4 = lowering jump, 8 = raising jump; CANON < 0 means the
+// kinds are decided at run time.
+template <bool REAL, bool TMA, int NTHR, int CANON>
+__global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassParams P,
+                                                   const __grid_constant__ CUtensorMap tmap,
+                                                   const double2 *__restrict__ X, const Epi E) {
+  constexpr int PT = NTHR;
+  constexpr int NW = NTHR / 32;
+  constexpr int MC = 64 / NW;
   constexpr int NST = TMA ? 3 : 2;   // pipeline stages
   extern __shared__ __align__(128) double2 sm[];
   double2 *gts = sm + NST * NEL;     // ngroups * 64, layout [g][col bits][row bits]
@@ -186,25 +193,26 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
     }
     unsigned rfix, cfix;
     tile_origin(t, n, lo, rfix, cfix);
-    // thread elements: rows lane, lane+32; columns w, w+16, w+32, w+48
     unsigned rl[2] = {(unsigned)lane, (unsigned)lane + 32u};
-    unsigned cl[4] = {(unsigned)w, (unsigned)w + 16u, (unsigned)w + 32u, (unsigned)w + 48u};
-    unsigned r[2], c[4];
+    unsigned cl[MC];
+#pragma unroll
+    for (int m = 0; m < MC; m++) cl[m] = (unsigned)(w + NW * m);
+    unsigned r[2], c[MC];
 #pragma unroll
     for (int i = 0; i < 2; i++) r[i] = rfix | (rl[i] << lo);
 #pragma unroll
-    for (int m = 0; m < 4; m++) c[m] = cfix | (cl[m] << lo);
-    double2 acc[2][4];
+    for (int m = 0; m < MC; m++) c[m] = cfix | (cl[m] << lo);
+    double2 acc[2][MC];
     if (P.accin) {
 #pragma unroll
       for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int m = 0; m < 4; m++) acc[i][m] = P.accin[(size_t)c[m] * D + r[i]];
+        for (int m = 0; m < MC; m++) acc[i][m] = P.accin[(size_t)c[m] * D + r[i]];
     } else {
 #pragma unroll
       for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int m = 0; m < 4; m++) acc[i][m] = make_double2(0.0, 0.0);
+        for (int m = 0; m < MC; m++) acc[i][m] = make_double2(0.0, 0.0);
     }
     if (P.diag) {
       // groups 0 and 1 vary inside the tile (lo == 0 here); the others are
@@ -221,7 +229,7 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         dri.x += gconst.x;
         dri.y += gconst.y;
 #pragma unroll
-        for (int m = 0; m < 4; m++) {
+        for (int m = 0; m < MC; m++) {
           double2 d = __ldg(P.dc + c[m]);
           d.x += dri.x;
           d.y += dri.y;
@@ -237,44 +245,48 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         }
       }
     }
-    if (REAL && P.ncanon) {
-      // canonical single-bit terms: partner offsets are compile-time constants
+    if (REAL && (CANON > 0 || (CANON < 0 && P.ncanon))) {
+      constexpr bool C_HL = CANON < 0 || (CANON & 1), C_HR = CANON < 0 || (CANON & 2);
+      constexpr bool C_GL = CANON < 0 || (CANON & 4), C_GU = CANON < 0 || (CANON & 8);
+      // canonical single-bit terms: partner offsets are compile-time
+      // constants; absent kinds are compiled out, zero coefficients are
+      // applied as zeros (no branches between terms)
 #pragma unroll
       for (int b = 0; b < 6; b++) {
         const unsigned f = 1u << b;
-        const double hl = P.hl[b], hr = P.hr[b], gl = P.gl[b], gu = P.gu[b];
-        if (hl != 0.0) {
+        if (C_HL) {
+          const double hl = P.hl[b];
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int m = 0; m < 4; m++) {
+            for (int m = 0; m < MC; m++) {
               const double2 p = cur[cl[m] * 64 + (rl[i] ^ f)];
               acc[i][m].x = fma(-hl, p.y, acc[i][m].x);
               acc[i][m].y = fma(hl, p.x, acc[i][m].y);
             }
         }
-        if (hr != 0.0) {
+        if (C_HR) {
+          const double hr = P.hr[b];
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int m = 0; m < 4; m++) {
+            for (int m = 0; m < MC; m++) {
               const double2 p = cur[(cl[m] ^ f) * 64 + rl[i]];
               acc[i][m].x = fma(-hr, p.y, acc[i][m].x);
               acc[i][m].y = fma(hr, p.x, acc[i][m].y);
             }
         }
-        if (gl != 0.0 || gu != 0.0) {
+        if (C_GL || C_GU) {
+          const double gl = C_GL ? P.gl[b] : 0.0, gu = C_GU ? P.gu[b] : 0.0;
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int m = 0; m < 4; m++) {
+            for (int m = 0; m < MC; m++) {
               const bool rb = rl[i] & f, cb = cl[m] & f;
-              if (rb == cb) {
-                const double g = rb ? gu : gl;
-                const double2 p = cur[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
-                acc[i][m].x = fma(g, p.x, acc[i][m].x);
-                acc[i][m].y = fma(g, p.y, acc[i][m].y);
-              }
+              const double g = (rb != cb) ? 0.0 : (rb ? gu : gl);
+              const double2 p = cur[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
+              acc[i][m].x = fma(g, p.x, acc[i][m].x);
+              acc[i][m].y = fma(g, p.y, acc[i][m].y);
             }
         }
       }
@@ -290,7 +302,7 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         if (REAL) {
           const double wv = neg ? -T.coef.y : T.coef.y;
 #pragma unroll
-          for (int m = 0; m < 4; m++) {
+          for (int m = 0; m < MC; m++) {
             const double2 p = cur[cl[m] * 64 + pr];
             acc[i][m].x = fma(-wv, p.y, acc[i][m].x);
             acc[i][m].y = fma(wv, p.x, acc[i][m].y);
@@ -298,14 +310,14 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         } else {
           const double2 wv = neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef;
 #pragma unroll
-          for (int m = 0; m < 4; m++) cfma2(acc[i][m], wv, cur[cl[m] * 64 + pr]);
+          for (int m = 0; m < MC; m++) cfma2(acc[i][m], wv, cur[cl[m] * 64 + pr]);
         }
       }
     }
     for (int e = k + P.nR; k < e; k++) {
       const PassTerm T = P.t[k];
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
+      for (int m = 0; m < MC; m++) {
         if ((c[m] & T.cmask) != T.cval) continue;
         const bool neg = __popc(c[m] & T.smask) & 1;
         const unsigned pc = cl[m] ^ T.fl;
@@ -332,7 +344,7 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         const int sr = __popc(r[i] & T.smask);
         const unsigned pr = rl[i] ^ T.fl;
 #pragma unroll
-        for (int m = 0; m < 4; m++) {
+        for (int m = 0; m < MC; m++) {
           if ((c[m] & T.cmask) != T.cval) continue;
           const bool neg = (sr + __popc(c[m] & T.smask)) & 1;
           const double2 p = cur[(cl[m] ^ T.fl) * 64 + pr];
@@ -353,7 +365,7 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
         if ((r[i] & T.cmask) != T.cval) continue;
         const int sr = __popc(r[i] & T.smask);
 #pragma unroll
-        for (int m = 0; m < 4; m++) {
+        for (int m = 0; m < MC; m++) {
           if ((c[m] & T.cmask) != T.cval) continue;
           const bool neg = (sr + __popc(c[m] & T.smask)) & 1;
           cfma2(acc[i][m], neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef, cur[cl[m] * 64 + rl[i]]);
@@ -370,7 +382,7 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
 #pragma unroll
       for (int i = 0; i < 2; i++) {
 #pragma unroll
-        for (int m = 0; m < 4; m++) {
+        for (int m = 0; m < MC; m++) {
           const bool okr = (r[i] & T.cmask) == T.cval, okc = (c[m] & T.cmask) == T.cval;
           size_t pidx;
           int sg;
@@ -395,7 +407,7 @@ __global__ void __launch_bounds__(PT, 1) k_qpass(const __grid_constant__ PassPar
 #pragma unroll
     for (int i = 0; i < 2; i++) {
 #pragma unroll
-      for (int m = 0; m < 4; m++) {
+      for (int m = 0; m < MC; m++) {
         const size_t idx = (size_t)c[m] * D + r[i];
         const double2 Kv = acc[i][m];
         if (!P.last) {
@@ -528,14 +540,56 @@ void encode_tma(const PassParams &pp, const double2 *x, CUtensorMap *map) {
   if (r != CUDA_SUCCESS) fail(9, "ERROR! cuTensorMapEncodeTiled failed (%d)\n", (int)r);
 }
 
-template <bool REAL, bool TMA>
-void set_smem_attr(size_t smem) {
+template <bool REAL, bool TMA, int NTHR, int CANON>
+void launch_pass(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e,
+                 int grid, size_t smem, cudaStream_t s) {
   static bool done = false;
   if (!done) {
-    QCUDA(cudaFuncSetAttribute(k_qpass<REAL, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
+    QCUDA(cudaFuncSetAttribute(k_qpass<REAL, TMA, NTHR, CANON>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     done = true;
   }
+  k_qpass<REAL, TMA, NTHR, CANON><<<grid, NTHR, smem, s>>>(pp, map, x, e);
+}
+
+template <int CANON>
+void launch_canon(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e,
+                  int grid, size_t smem, cudaStream_t s) {
+  launch_pass<true, true, 1024, CANON>(pp, map, x, e, grid, smem, s);
+}
+
+// canonical fast path: real mode, TMA, no general terms in this pass
+void launch_canon_mask(int mask, const PassParams &pp, const CUtensorMap &map, const double2 *x,
+                       const Epi &e, int grid, size_t smem, cudaStream_t s) {
+  switch (mask) {
+    case 0: launch_canon<0>(pp, map, x, e, grid, smem, s); break;
+    case 1: launch_canon<1>(pp, map, x, e, grid, smem, s); break;
+    case 2: launch_canon<2>(pp, map, x, e, grid, smem, s); break;
+    case 3: launch_canon<3>(pp, map, x, e, grid, smem, s); break;
+    case 4: launch_canon<4>(pp, map, x, e, grid, smem, s); break;
+    case 5: launch_canon<5>(pp, map, x, e, grid, smem, s); break;
+    case 6: launch_canon<6>(pp, map, x, e, grid, smem, s); break;
+    case 7: launch_canon<7>(pp, map, x, e, grid, smem, s); break;
+    case 8: launch_canon<8>(pp, map, x, e, grid, smem, s); break;
+    case 9: launch_canon<9>(pp, map, x, e, grid, smem, s); break;
+    case 10: launch_canon<10>(pp, map, x, e, grid, smem, s); break;
+    case 11: launch_canon<11>(pp, map, x, e, grid, smem, s); break;
+    case 12: launch_canon<12>(pp, map, x, e, grid, smem, s); break;
+    case 13: launch_canon<13>(pp, map, x, e, grid, smem, s); break;
+    case 14: launch_canon<14>(pp, map, x, e, grid, smem, s); break;
+    default: launch_canon<15>(pp, map, x, e, grid, smem, s); break;
+  }
+}
+
+int canon_mask(const PassParams &pp) {
+  int m = 0;
+  for (int b = 0; b < 6; b++) {
+    if (pp.hl[b] != 0) m |= 1;
+    if (pp.hr[b] != 0) m |= 2;
+    if (pp.gl[b] != 0) m |= 4;
+    if (pp.gu[b] != 0) m |= 8;
+  }
+  return m;
 }
 
 }  // namespace
@@ -674,10 +728,13 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
     const bool tma = pp.tma != 0;
     if (tma) encode_tma(pp, x, &map);
     const size_t smem = (size_t)((tma ? 3 : 2) * NEL + QMAX_GROUPS * 64) * sizeof(double2);
-    if (pp.real && tma) { set_smem_attr<true, true>(smem); k_qpass<true, true><<<grid, PT, smem, s>>>(pp, map, x, e); }
-    else if (pp.real) { set_smem_attr<true, false>(smem); k_qpass<true, false><<<grid, PT, smem, s>>>(pp, map, x, e); }
-    else if (tma) { set_smem_attr<false, true>(smem); k_qpass<false, true><<<grid, PT, smem, s>>>(pp, map, x, e); }
-    else { set_smem_attr<false, false>(smem); k_qpass<false, false><<<grid, PT, smem, s>>>(pp, map, x, e); }
+    const bool only_canon = pp.real && tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 &&
+                            pp.nJx == 0 && pp.nspill == 0;
+    if (only_canon) launch_canon_mask(canon_mask(pp), pp, map, x, e, grid, smem, s);
+    else if (pp.real && tma) launch_pass<true, true, 512, -1>(pp, map, x, e, grid, smem, s);
+    else if (pp.real) launch_pass<true, false, 512, -1>(pp, map, x, e, grid, smem, s);
+    else if (tma) launch_pass<false, true, 512, -1>(pp, map, x, e, grid, smem, s);
+    else launch_pass<false, false, 512, -1>(pp, map, x, e, grid, smem, s);
     count_launch();
     QCUDA(cudaGetLastError());
   }

@@ -1,0 +1,3 @@
+/* Drop-in header: QuaC programs include solver.h; everything this engine
+ * provides is declared in quac_b200.h. */
+#include "../quac_b200.h"

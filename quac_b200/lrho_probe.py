@@ -1,0 +1,39 @@
+"""Applies L.rho a few times on the device (for profiling runs).
+
+    python -m quac_b200.lrho_probe --qubits 12 --reps 3 [--path 0|1|2]
+
+Builds the open transverse-field Ising chain of the benchmark with the
+given number of qubits, allocates x and y with torch on cuda:0 and calls
+quac_lrho_apply_device `reps` times.
+"""
+import argparse
+
+import torch
+
+import quac_b200 as q
+from quac_b200.systems import Builder, tfim
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--qubits", type=int, default=12)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--path", type=int, default=0)
+    a = ap.parse_args()
+    q.lib()
+    q.QuaC_initialize()
+    q.set_kernel_path(a.path)
+    S = Builder(q)
+    tfim(S, a.qubits)
+    q.construct_matrix(S.qs)
+    n = S.D * S.D
+    x = torch.randn(n, dtype=torch.complex128, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(a.reps):
+        q.lrho_apply_device(S.qs, x.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    print(f"ok D={S.D} reps={a.reps} launches={q.kernel_launch_count()}")
+
+
+if __name__ == "__main__":
+    main()

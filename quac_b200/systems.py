@@ -1,0 +1,97 @@
+"""Synthetic workloads of the benchmarks and parity tests.
+
+Each builder takes an object ``S`` offering ``op(levels)`` (returning an
+operator family with a / dag / n / eye / sig_x / sig_y / sig_z), ``ham(a,
+*ops)`` and ``lin(a, *ops)`` -- :class:`Builder` below drives this package,
+the CPU oracle's ``OSys`` drives the oracle -- so both receive the same
+term list.  Parameters are drawn from seeded numpy generators.
+"""
+import numpy as np
+
+
+class Builder:
+    """Builds a system through this package's QuaC-style API."""
+
+    def __init__(self, q=None):
+        if q is None:
+            import quac_b200 as q
+        self.q = q
+        self.qs = q.initialize_system()
+        self.levels = []
+
+    def op(self, levels):
+        self.levels.append(levels)
+        return self.q.create_op_sys(self.qs, levels)
+
+    def vec(self, levels):
+        self.levels.append(levels)
+        return self.q.create_vec_op_sys(self.qs, levels)
+
+    def ham(self, a, *ops):
+        self.q.add_ham_term(self.qs, a, *ops)
+
+    def lin(self, a, *ops):
+        self.q.add_lin_term(self.qs, a, *ops)
+
+    @property
+    def D(self):
+        return int(np.prod(self.levels))
+
+
+def jc(S, nc=10, g=0.1, kappa=1e-2, gamma=1e-3):
+    """Jaynes-Cummings: emitter (2) created first, cavity (nc) second,
+    H = g (a^dag sigma + a sigma^dag), L = kappa a, gamma sigma."""
+    qb = S.op(2)
+    cav = S.op(nc)
+    S.ham(g, cav.dag, qb.a)
+    S.ham(g, cav.a, qb.dag)
+    S.lin(kappa, cav.a)
+    S.lin(gamma, qb.a)
+    return qb, cav
+
+
+def driven_jc(S, nc, delta, g, omega, kappa, gamma=1e-3):
+    """Driven JC: H = delta a^dag a + g (a^dag sigma + a sigma^dag) + omega (a + a^dag)."""
+    qb = S.op(2)
+    cav = S.op(nc)
+    S.ham(delta, cav.n)
+    S.ham(g, cav.dag, qb.a)
+    S.ham(g, cav.a, qb.dag)
+    S.ham(omega, cav.a)
+    S.ham(omega, cav.dag)
+    S.lin(kappa, cav.a)
+    S.lin(gamma, qb.a)
+    return qb, cav
+
+
+def tfim(S, n, seed=3, g1=1e-3, gphi=5e-4):
+    """Open transverse-field Ising chain: sum J_i Z_i Z_{i+1} + sum h_i X_i with
+    J ~ U[0.5, 1.5], h ~ N(0, 0.2^2); decay g1 and dephasing gphi per qubit."""
+    rng = np.random.default_rng(seed)
+    J = rng.uniform(0.5, 1.5, size=n - 1)
+    h = rng.normal(0.0, 0.2, size=n)
+    qs = [S.op(2) for _ in range(n)]
+    for i in range(n - 1):
+        S.ham(J[i], qs[i].sig_z, qs[i + 1].sig_z)
+    for i in range(n):
+        S.ham(h[i], qs[i].sig_x)
+    for i in range(n):
+        S.lin(g1, qs[i].a)
+        S.lin(gphi, qs[i].n)
+    return qs
+
+
+def tavis_cummings(S, ne=6, nc=8, omega=0.3, delta=0.5, kappa=0.1, gamma=5e-3, g=0.1):
+    """Driven Tavis-Cummings: ne two-level emitters and a cavity of nc levels."""
+    ems = [S.op(2) for _ in range(ne)]
+    cav = S.op(nc)
+    S.ham(delta, cav.n)
+    for e in ems:
+        S.ham(g, cav.dag, e.a)
+        S.ham(g, cav.a, e.dag)
+    S.ham(omega, cav.a)
+    S.ham(omega, cav.dag)
+    S.lin(kappa, cav.a)
+    for e in ems:
+        S.lin(gamma, e.a)
+    return ems, cav

@@ -34,59 +34,7 @@ class ProductSystem:
         return int(np.prod(self.levels))
 
 
-def jc(S, nc=10, g=0.1, kappa=1e-2, gamma=1e-3):
-    """Jaynes-Cummings: emitter (2) created first, cavity (nc) second."""
-    qb = S.op(2)
-    cav = S.op(nc)
-    S.ham(g, cav.dag, qb.a)
-    S.ham(g, cav.a, qb.dag)
-    S.lin(kappa, cav.a)
-    S.lin(gamma, qb.a)
-    return qb, cav
-
-
-def driven_jc(S, nc, delta, g, omega, kappa, gamma=1e-3):
-    qb = S.op(2)
-    cav = S.op(nc)
-    S.ham(delta, cav.n)
-    S.ham(g, cav.dag, qb.a)
-    S.ham(g, cav.a, qb.dag)
-    S.ham(omega, cav.a)
-    S.ham(omega, cav.dag)
-    S.lin(kappa, cav.a)
-    S.lin(gamma, qb.a)
-    return qb, cav
-
-
-def tfim(S, n, seed=3, g1=1e-3, gphi=5e-4):
-    """Open transverse-field Ising chain: sum J ZZ + sum h X, T1/T2 per qubit."""
-    rng = np.random.default_rng(seed)
-    J = rng.uniform(0.5, 1.5, size=n - 1)
-    h = rng.normal(0.0, 0.2, size=n)
-    qs = [S.op(2) for _ in range(n)]
-    for i in range(n - 1):
-        S.ham(J[i], qs[i].sig_z, qs[i + 1].sig_z)
-    for i in range(n):
-        S.ham(h[i], qs[i].sig_x)
-    for i in range(n):
-        S.lin(g1, qs[i].a)
-        S.lin(gphi, qs[i].n)
-    return qs
-
-
-def tavis_cummings(S, ne=6, nc=8, omega=0.3, delta=0.5, kappa=0.1, gamma=5e-3, g=0.1):
-    ems = [S.op(2) for _ in range(ne)]
-    cav = S.op(nc)
-    S.ham(delta, cav.n)
-    for e in ems:
-        S.ham(g, cav.dag, e.a)
-        S.ham(g, cav.a, e.dag)
-    S.ham(omega, cav.a)
-    S.ham(omega, cav.dag)
-    S.lin(kappa, cav.a)
-    for e in ems:
-        S.lin(gamma, e.a)
-    return ems, cav
+from quac_b200.systems import driven_jc, jc, tavis_cummings, tfim  # noqa: F401,E402
 
 
 def mixed(S):

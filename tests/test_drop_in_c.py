@@ -1,0 +1,47 @@
+"""A QuaC-style C program builds unchanged against include/quac/*.h and
+links libquac_b200.so (CPU); on a GPU it runs and matches the oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def _build(tmp_path):
+    exe = tmp_path / "jc_drop_in"
+    libdir = os.path.join(ROOT, "quac_b200")
+    cmd = ["/usr/bin/gcc", "-std=c99", "-O2", "-Wall", "-I", os.path.join(ROOT, "include", "quac"),
+           os.path.join(ROOT, "tests", "c", "jc_drop_in.c"), "-o", str(exe), "-L", libdir,
+           "-lquac_b200", f"-Wl,-rpath,{libdir}", "-lm"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_c_program_compiles_and_links(quac, tmp_path):
+    _build(tmp_path)
+
+
+@pytest.mark.gpu
+def test_c_program_runs_and_matches_oracle(quac, oracle, tmp_path):
+    exe = _build(tmp_path)
+    r = subprocess.run([str(exe), "-ts_rk_type", "4", "-ts_adapt_type", "none"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    vals = {ln.split()[0]: float(ln.split()[1]) for ln in r.stdout.splitlines()
+            if ln.startswith(("final_", "trace"))}
+    steps = [ln.split() for ln in r.stdout.splitlines() if ln.startswith("step ")]
+    assert [int(s[1]) for s in steps] == list(range(0, 201, 50))
+    S = oracle.OSys()
+    from quac_b200.systems import jc
+    jc(S)
+    h = S.csr_handle()
+    x0 = np.zeros(400, dtype=complex)
+    x0[10 * 20 + 10] = 1.0
+    y = oracle.rk4(h, x0, 0.01, 200)
+    oracle.free_csr(h)
+    assert abs(vals["final_qb"] - oracle.expect_dm([2, 10], y, (0, 0, -1)).real) < 1e-12
+    assert abs(vals["final_cav"] - oracle.expect_dm([2, 10], y, (0, 1, -1)).real) < 1e-12
+    assert abs(vals["trace"] - 1.0) < 1e-12

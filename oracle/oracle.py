@@ -58,6 +58,8 @@ def lib():
         L.orc_rk4.argtypes = [vp, vp, dbl, i64]
         L.orc_bs3.restype = i64
         L.orc_bs3.argtypes = [vp, vp, dbl, dbl, dbl, dbl, dbl, dbl, dbl, i64, vp]
+        L.orc_dp5.restype = i64
+        L.orc_dp5.argtypes = [vp, vp, dbl, dbl, dbl, dbl, dbl, dbl, dbl, i64, vp]
         L.orc_expect_dm.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, vp, vp]
         L.orc_expect_wf.argtypes = [ctypes.c_int, vp, ctypes.c_int, vp, vp, vp]
         L.orc_gate_superop.argtypes = [ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, dbl, dbl,
@@ -183,6 +185,14 @@ def bs3(h, y0, t0, tmax, dt0, atol=5e-7, rtol=5e-7, hmin=0.01, hmax=1.0, max_ste
     y = np.array(y0, dtype=np.complex128, copy=True)
     nrej = ctypes.c_int64(0)
     nacc = lib().orc_bs3(h, _p(y), t0, tmax, dt0, atol, rtol, hmin, hmax, max_steps,
+                         ctypes.byref(nrej))
+    return y, nacc, nrej.value
+
+
+def dp5(h, y0, t0, tmax, dt0, atol=5e-7, rtol=5e-7, hmin=0.01, hmax=1.0, max_steps=10 ** 9):
+    y = np.array(y0, dtype=np.complex128, copy=True)
+    nrej = ctypes.c_int64(0)
+    nacc = lib().orc_dp5(h, _p(y), t0, tmax, dt0, atol, rtol, hmin, hmax, max_steps,
                          ctypes.byref(nrej))
     return y, nacc, nrej.value
 

@@ -424,6 +424,74 @@ i64 orc_bs3(const csr *A, double *yd, double t0, double tmax, double dt0, double
   return acc;
 }
 
+/* Dormand-Prince 5(4) (the published 1980 tableau, FSAL) with the same
+ * basic controller as orc_bs3 (exponent -1/5).  The error norm is the
+ * weighted RMS of h*sum (b - bhat)_i k_i. */
+static const double DP_C[7] = {0.0, 0.2, 0.3, 0.8, 8.0 / 9.0, 1.0, 1.0};
+static const double DP_A[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {0.2, 0, 0, 0, 0, 0},
+    {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0, 0},
+    {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0},
+    {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0},
+    {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0},
+    {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+static const double DP_E[7] = {35.0 / 384.0 - 5179.0 / 57600.0, 0.0, 500.0 / 1113.0 - 7571.0 / 16695.0,
+                               125.0 / 192.0 - 393.0 / 640.0, -2187.0 / 6784.0 + 92097.0 / 339200.0,
+                               11.0 / 84.0 - 187.0 / 2100.0, -1.0 / 40.0};
+
+i64 orc_dp5(const csr *A, double *yd, double t0, double tmax, double dt0, double atol,
+            double rtol, double hmin, double hmax, i64 max_steps, i64 *nrej) {
+  i64 n = A->nrows;
+  cplx *y = (cplx *)yd;
+  cplx *k[7];
+  for (int s = 0; s < 7; s++) k[s] = malloc(n * sizeof(cplx));
+  cplx *x = malloc(n * sizeof(cplx));
+  double t = t0, h = dt0;
+  i64 acc = 0, rej = 0;
+  while (t < tmax - 1e-12 * fabs(tmax) && acc < max_steps) {
+    int last = 0;
+    if (t + h >= tmax) { h = tmax - t; last = 1; }
+    orc_spmv(A, (double *)y, (double *)k[0]);
+    for (int s = 1; s < 7; s++) {
+      for (i64 i = 0; i < n; i++) {
+        cplx v = y[i];
+        for (int j = 0; j < s; j++) v += h * DP_A[s][j] * k[j][i];
+        x[i] = v;
+      }
+      orc_spmv(A, (double *)x, (double *)k[s]);
+    }
+    /* x holds the 5th-order solution (stage 7 input) */
+    double ssum = 0;
+    for (i64 i = 0; i < n; i++) {
+      cplx e = 0;
+      for (int j = 0; j < 7; j++) e += h * DP_E[j] * k[j][i];
+      double m = fmax(cabs(y[i]), cabs(x[i]));
+      double q = cabs(e) / (atol + rtol * m);
+      ssum += q * q;
+    }
+    double err = sqrt(ssum / (double)n);
+    double fac = (err > 0) ? 0.9 * pow(err, -0.2) : 10.0;
+    if (fac < 0.1) fac = 0.1;
+    if (fac > 10.0) fac = 10.0;
+    double hnew = h * fac;
+    if (hnew < hmin) hnew = hmin;
+    if (hnew > hmax) hnew = hmax;
+    if (err <= 1.0 || h <= hmin * (1 + 1e-12)) {
+      memcpy(y, x, n * sizeof(cplx));
+      t = last ? tmax : t + h;
+      acc++;
+    } else {
+      rej++;
+    }
+    h = hnew;
+  }
+  if (nrej) *nrej = rej;
+  for (int s = 0; s < 7; s++) free(k[s]);
+  free(x);
+  return acc;
+}
+
 /* ------------------------------------------------------------ observables */
 /* Tr(O rho) for O = ops[0]*ops[1]*...: qvec_utilities.c:1197-1283.
  * Sum over columns c of O[c, j(c)] * rho[j(c), c]. */

@@ -164,5 +164,15 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
 // Reads and clears the program's device error word; reports through fail().
 bool check_program_error(DeviceProgram &P, cudaStream_t s);
 void zero_epi(Epi &e);
+// lincomb.cu
+void launch_lincomb(double2 *out, const double2 *base, int nin, const double2 *const *in,
+                    const double *coef, int64_t n, cudaStream_t s);
+void launch_lincomb_norm(const double2 *base, const double2 *ref, int nin, const double2 *const *in,
+                         const double *coef, int64_t n, double atol, double rtol, double *nsum,
+                         cudaStream_t s);
+// Dormand-Prince 5(4) tableau (published 1980 coefficients)
+extern const double kDP_C[7];
+extern const double kDP_A[7][6];
+extern const double kDP_E[7];
 
 }  // namespace quac

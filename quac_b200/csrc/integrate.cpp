@@ -14,6 +14,19 @@
 
 namespace quac {
 
+const double kDP_C[7] = {0.0, 0.2, 0.3, 0.8, 8.0 / 9.0, 1.0, 1.0};
+const double kDP_A[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {0.2, 0, 0, 0, 0, 0},
+    {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0, 0},
+    {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0},
+    {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0},
+    {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0},
+    {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+const double kDP_E[7] = {35.0 / 384.0 - 5179.0 / 57600.0, 0.0, 500.0 / 1113.0 - 7571.0 / 16695.0,
+                         125.0 / 192.0 - 393.0 / 640.0, -2187.0 / 6784.0 + 92097.0 / 339200.0,
+                         11.0 / 84.0 - 187.0 / 2100.0, -1.0 / 40.0};
+
 void apply_gate_superop(qsystem qs, const struct quantum_gate_struct &g, Vec v, bool is_dm,
                         cudaStream_t s);
 void apply_gate_inplace(qvec q, const struct quantum_gate_struct &g, cudaStream_t s);
@@ -96,9 +109,10 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
   if (o.max_steps > 0) steps_max = o.max_steps;
   const bool fixed = (o.rk_type == "4") || (o.adapt_type == "none");
   const bool rk4 = (o.rk_type == "4");
+  const bool dp5 = (o.rk_type == "5dp");
   cudaStream_t s = stream_of(qs);
   Workspace &W = qs->impl->ws;
-  W.ensure(n, 4);
+  W.ensure(n, dp5 ? 8 : 4);
   vec_sync_to_device(v);
   QCUDA(cudaDeviceSynchronize());
 
@@ -129,7 +143,43 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
     double2 *y = v->d;
     bool accepted = true;
     double h_next = h;
-    if (fixed && rk4 && !o.rk4_classic) {
+    if (dp5) {
+      // Dormand-Prince 5(4): K_s = L x_s (one launch each), stage inputs and
+      // the error norm by fused linear combinations of the stored K's
+      double2 *K[7] = {W.bufs[0], W.bufs[1], W.bufs[2], W.bufs[3], W.bufs[4], W.bufs[5], W.bufs[6]};
+      double2 *xs = W.bufs[7];
+      for (int st_i = 0; st_i < 7; st_i++) {
+        const double2 *X = y;
+        if (st_i > 0) {
+          double c[6];
+          for (int j = 0; j < st_i; j++) c[j] = h_try * kDP_A[st_i][j];
+          launch_lincomb(xs, y, st_i, (const double2 *const *)K, c, n, s);
+          X = xs;
+        }
+        Epi e;
+        zero_epi(e);
+        e.kout = K[st_i];
+        launch_lrho_any(PP, X, e, s);
+      }
+      // xs now holds the fifth-order solution (input of stage 7)
+      double c[7];
+      for (int j = 0; j < 7; j++) c[j] = h_try * kDP_E[j];
+      if (fixed) {
+        std::swap(v->d, W.bufs[7]);
+      } else {
+        QCUDA(cudaMemsetAsync(W.dsum, 0, sizeof(double), s));
+        launch_lincomb_norm(y, xs, 7, (const double2 *const *)K, c, n, o.atol, o.rtol, W.dsum, s);
+        QCUDA(cudaMemcpyAsync(W.hsum, W.dsum, sizeof(double), cudaMemcpyDeviceToHost, s));
+        QCUDA(cudaStreamSynchronize(s));
+        const double err = std::sqrt(W.hsum[0] / (double)n);
+        double fac = err > 0 ? 0.9 * std::pow(err, -0.2) : 10.0;
+        fac = std::min(10.0, std::max(0.1, fac));
+        h_next = std::min(hmax, std::max(hmin, h_try * fac));
+        accepted = (err <= 1.0) || (h_try <= hmin * (1 + 1e-12));
+        if (accepted) std::swap(v->d, W.bufs[7]);
+        if (!accepted) { h = h_next; continue; }
+      }
+    } else if (fixed && rk4 && !o.rk4_classic) {
       // For a time-independent linear right-hand side the classical RK4 step
       // equals the degree-4 Taylor polynomial of exp(hL); evaluated by
       // Horner's rule each stage reads one vector besides its input:

@@ -1,0 +1,98 @@
+// Linear combinations of stage vectors for the multi-stage integrators:
+//   out[i] = base[i] + sum_j coef[j] * in_j[i]            (up to 8 inputs)
+// optionally accumulating the weighted error norm of the combination
+//   sum_i (|out_i - base_i| / (atol + rtol * max(|base_i|, |ref_i|)))^2
+// (mode 1: out is not written, only the norm of sum_j coef_j in_j is taken
+// against base and ref).
+#include "common.h"
+
+namespace quac {
+
+namespace {
+
+constexpr int NT = 256;
+
+struct LinArgs {
+  const double2 *in[8];
+  double coef[8];
+  int nin;
+  const double2 *base;
+  double2 *out;
+  const double2 *ref;  // second vector of the error weight (norm mode)
+  double atol, rtol;
+  double *nsum;        // norm accumulator (norm mode)
+};
+
+__global__ void k_lincomb(const LinArgs A, int64_t n) {
+  __shared__ double red[NT / 32];
+  double loc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      if (j < A.nin) {
+        const double2 v = A.in[j][i];
+        s.x = fma(A.coef[j], v.x, s.x);
+        s.y = fma(A.coef[j], v.y, s.y);
+      }
+    }
+    if (A.nsum) {
+      const double2 b = A.base[i], r = A.ref[i];
+      const double m = fmax(sqrt(b.x * b.x + b.y * b.y), sqrt(r.x * r.x + r.y * r.y));
+      const double q = sqrt(s.x * s.x + s.y * s.y) / (A.atol + A.rtol * m);
+      loc += q * q;
+    } else {
+      const double2 b = A.base ? A.base[i] : make_double2(0.0, 0.0);
+      A.out[i] = make_double2(b.x + s.x, b.y + s.y);
+    }
+  }
+  if (A.nsum) {
+    for (int o = 16; o > 0; o >>= 1) loc += __shfl_down_sync(0xffffffffu, loc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = loc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; w++) t += red[w];
+      atomicAdd(A.nsum, t);
+    }
+  }
+}
+
+int grid_of(int64_t n) {
+  int64_t b = (n + NT - 1) / NT;
+  return (int)(b < 148 * 16 ? b : 148 * 16);
+}
+
+}  // namespace
+
+void launch_lincomb(double2 *out, const double2 *base, int nin, const double2 *const *in,
+                    const double *coef, int64_t n, cudaStream_t s) {
+  LinArgs A;
+  memset(&A, 0, sizeof(A));
+  A.nin = nin;
+  for (int j = 0; j < nin; j++) { A.in[j] = in[j]; A.coef[j] = coef[j]; }
+  A.base = base;
+  A.out = out;
+  k_lincomb<<<grid_of(n), NT, 0, s>>>(A, n);
+  count_launch();
+  QCUDA(cudaGetLastError());
+}
+
+void launch_lincomb_norm(const double2 *base, const double2 *ref, int nin, const double2 *const *in,
+                         const double *coef, int64_t n, double atol, double rtol, double *nsum,
+                         cudaStream_t s) {
+  LinArgs A;
+  memset(&A, 0, sizeof(A));
+  A.nin = nin;
+  for (int j = 0; j < nin; j++) { A.in[j] = in[j]; A.coef[j] = coef[j]; }
+  A.base = base;
+  A.ref = ref;
+  A.atol = atol;
+  A.rtol = rtol;
+  A.nsum = nsum;
+  k_lincomb<<<grid_of(n), NT, 0, s>>>(A, n);
+  count_launch();
+  QCUDA(cudaGetLastError());
+}
+
+}  // namespace quac

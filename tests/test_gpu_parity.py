@@ -123,6 +123,38 @@ def test_bs3_adaptive_matches_oracle(quac, oracle):
     S.qs.destroy()
 
 
+@pytest.mark.parametrize("adapt", ["basic", "none"])
+def test_dp5_matches_oracle(quac, oracle, adapt):
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.driven_jc(S, 8, 0.3, 0.2, 0.1, 0.05)
+    H.driven_jc(O, 8, 0.3, 0.2, 0.1, 0.05)
+    quac.construct_matrix(S.qs)
+    rho = quac.create_qvec_sys(S.qs)
+    D = S.D
+    quac.add_to_qvec(rho, 1.0, 8, 8)
+    quac.assemble_qvec(rho)
+    quac.set_ts_options(rk_type="5dp", adapt_type=adapt)
+    try:
+        quac.time_step_sys(S.qs, rho, 0.0, 3.0, 0.05, 100000)
+    finally:
+        quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+    y = rho.to_numpy()
+    h = O.csr_handle()
+    x0 = np.zeros(D * D, dtype=complex)
+    x0[8 * D + 8] = 1.0
+    if adapt == "basic":
+        yo, nacc, nrej = oracle.dp5(h, x0, 0.0, 3.0, 0.05)
+    else:
+        # fixed step: the controller accepts everything (hmin = hmax = dt)
+        yo, nacc, nrej = oracle.dp5(h, x0, 0.0, 3.0, 0.05, atol=1e300, hmin=0.05, hmax=0.05)
+        assert nacc == 60 and nrej == 0
+    oracle.free_csr(h)
+    assert _rel(y, yo) < 1e-10
+    rho.destroy()
+    S.qs.destroy()
+
+
 def test_t1_decay_known_answer_gpu(quac):
     q = quac
     qs = q.initialize_system()

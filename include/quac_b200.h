@@ -254,6 +254,18 @@ PetscInt steady_state_sys(qsystem qsys, qvec x);
 int quac_lrho_apply_device(qsystem qsys, const void *x_dev, void *y_dev);
 /* Same on host buffers: copies x in, applies L, copies y out. */
 int quac_lrho_apply_host(qsystem qsys, const PetscScalar *x_host, PetscScalar *y_host);
+/* No reference counterpart.  quac_lrho_apply_device without any device
+ * allocation at call time, for callers that must not allocate inside their
+ * loop: a framework whose memory pool already holds the device's memory, or
+ * a tight control loop where cudaFree's device-wide synchronisation would
+ * stall other streams.  The multi-pass kernel's D^2 running sum lives in a
+ * fixed 16 MiB device array, so qsys->dim may be at most 2^20 (10 qubits);
+ * larger systems return an error.  Call quac_lrho_noalloc_setup(qsys) once,
+ * with the system's device current, before the first apply and before any
+ * stream capture.  All systems on a device share the one array: calls that
+ * overlap in time race and must be serialised by the caller. */
+int quac_lrho_noalloc_setup(qsystem qsys);
+int quac_lrho_apply_device_noalloc(qsystem qsys, const void *x_dev, void *y_dev);
 /* Time-steps host data in place: one call = H2D + integration + D2H. */
 int quac_time_step_host(qsystem qsys, PetscScalar *x_host, PetscReal t0, PetscReal tmax,
                         PetscReal dt, PetscInt steps_max);

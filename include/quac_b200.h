@@ -266,6 +266,40 @@ int quac_lrho_apply_host(qsystem qsys, const PetscScalar *x_host, PetscScalar *y
  * overlap in time race and must be serialised by the caller. */
 int quac_lrho_noalloc_setup(qsystem qsys);
 int quac_lrho_apply_device_noalloc(qsystem qsys, const void *x_dev, void *y_dev);
+/* Batched ensembles (no reference counterpart: QuaC integrates one system
+ * per time_step_sys call, qsystem.c:895-1098).  Many independent systems,
+ * each built with the usual calls (initialize_system, create_op_sys,
+ * add_ham_term, add_lin_term), are integrated together as density matrices
+ * in one persistent launch, each with its own adaptive Dormand-Prince 5(4)
+ * step (the -ts_rk_type 5dp controller of time_step_sys).  The states are
+ * one packed array: instance i occupies D_i^2 column-stacked values from
+ * quac_ensemble_state_offset(ens, i). */
+typedef struct quac_ensemble_s *quac_ensemble;
+int quac_ensemble_create(quac_ensemble *ens, int64_t n, const qsystem *systems);
+int quac_ensemble_destroy(quac_ensemble ens);
+/* precision 0: complex128 throughout; 1: complex64 right-hand-side
+ * increments with the complex128 state and controller.  Defaults: 0,
+ * atol = rtol = 5e-7, step limits [0.01, 1], 10^6 steps. */
+int quac_ensemble_set_options(quac_ensemble ens, int precision, double atol, double rtol, double hmin,
+                              double hmax, int64_t max_steps);
+/* Launch shape: warps per CTA (4, 8, 16, 32), CTAs per SM, target density
+ * matrix elements per thread (sets how many warps share an instance). */
+int quac_ensemble_set_shape(quac_ensemble ens, int warps, int ctas_per_sm, int elems_per_thread);
+int quac_ensemble_get_shape(quac_ensemble ens, int *warps, int *ctas_per_sm, int *elems_per_thread);
+/* Times every launch shape on a short run t0 .. t0 + t_probe, keeps the
+ * fastest and leaves the states unchanged. */
+int quac_ensemble_tune(quac_ensemble ens, double t0, double t_probe, double dt0, double *best_ms);
+int64_t quac_ensemble_state_offset(quac_ensemble ens, int64_t i);
+void *quac_ensemble_state_device_ptr(quac_ensemble ens);
+int quac_ensemble_set_states(quac_ensemble ens, const PetscScalar *rho);
+int quac_ensemble_get_states(quac_ensemble ens, PetscScalar *rho);
+/* Integrates every instance from t0 to tmax (first step dt0); fails if an
+ * instance hit the step limit or a non-finite error norm. */
+int quac_ensemble_run(quac_ensemble ens, double t0, double tmax, double dt0);
+int quac_ensemble_get_stats(quac_ensemble ens, int64_t i, double *t, int64_t *steps, int64_t *rejected,
+                            int *flags);
+/* Re(diag rho_i) of every instance, packed: D_0 values, then D_1, ... */
+int quac_ensemble_populations(quac_ensemble ens, double *pops);
 /* Time-steps host data in place: one call = H2D + integration + D2H. */
 int quac_time_step_host(qsystem qsys, PetscScalar *x_host, PetscReal t0, PetscReal tmax,
                         PetscReal dt, PetscInt steps_max);

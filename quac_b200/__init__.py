@@ -168,6 +168,19 @@ def lib():
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "read_qvec_wf_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "print_qvec_file": (None, [P(_QvecStruct), ctypes.c_char_p]),
+        "quac_ensemble_create": (ctypes.c_int, [P(vp), i64, P(P(_QsysStruct))]),
+        "quac_ensemble_destroy": (ctypes.c_int, [vp]),
+        "quac_ensemble_set_options": (ctypes.c_int, [vp, ctypes.c_int, dbl, dbl, dbl, dbl, i64]),
+        "quac_ensemble_set_shape": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+        "quac_ensemble_get_shape": (ctypes.c_int, [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]),
+        "quac_ensemble_tune": (ctypes.c_int, [vp, dbl, dbl, dbl, P(dbl)]),
+        "quac_ensemble_state_offset": (i64, [vp, i64]),
+        "quac_ensemble_state_device_ptr": (vp, [vp]),
+        "quac_ensemble_set_states": (ctypes.c_int, [vp, vp]),
+        "quac_ensemble_get_states": (ctypes.c_int, [vp, vp]),
+        "quac_ensemble_run": (ctypes.c_int, [vp, dbl, dbl, dbl]),
+        "quac_ensemble_get_stats": (ctypes.c_int, [vp, i64, P(dbl), P(i64), P(i64), P(ctypes.c_int)]),
+        "quac_ensemble_populations": (ctypes.c_int, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -630,3 +643,92 @@ def set_stream(qs, stream_ptr):
 def set_kernel_path(path):
     """0: default selection; 1: generic table kernel; 2: single-pass bit-mask kernel."""
     lib().quac_set_kernel_path(int(path))
+
+
+# ---------------------------------------------------------------- ensembles
+class Ensemble:
+    """Many independent systems integrated together (quac_ensemble_*).
+
+    ``systems`` are QSystem objects with their terms added; the ensemble
+    copies their compiled terms, so they may be destroyed afterwards.
+    States are one packed complex128 array (instance i at ``offsets[i]``,
+    D_i^2 column-stacked values)."""
+
+    def __init__(self, systems):
+        systems = list(systems)
+        n = len(systems)
+        arr = (ctypes.POINTER(_QsysStruct) * n)(*[s._ptr for s in systems])
+        h = vp()
+        rc = lib().quac_ensemble_create(ctypes.byref(h), n, arr)
+        _check()
+        if rc:
+            raise QuacError("quac_ensemble_create failed")
+        self._h = h
+        self.n = n
+        self.offsets = np.array([lib().quac_ensemble_state_offset(h, i) for i in range(n + 1)], dtype=np.int64)
+        self.dims = np.rint(np.sqrt(np.diff(self.offsets))).astype(np.int64)
+
+    def _call(self, name, *args):
+        rc = getattr(lib(), name)(self._h, *args)
+        _check()
+        if rc:
+            raise QuacError(f"{name} failed")
+
+    def set_options(self, precision=0, atol=5e-7, rtol=5e-7, hmin=0.01, hmax=1.0, max_steps=10 ** 6):
+        self._call("quac_ensemble_set_options", precision, atol, rtol, hmin, hmax, max_steps)
+
+    def set_shape(self, warps, ctas_per_sm, elems_per_thread):
+        self._call("quac_ensemble_set_shape", warps, ctas_per_sm, elems_per_thread)
+
+    def shape(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._call("quac_ensemble_get_shape", ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+    def tune(self, t0, t_probe, dt0):
+        ms = dbl()
+        self._call("quac_ensemble_tune", t0, t_probe, dt0, ctypes.byref(ms))
+        return ms.value
+
+    def set_states(self, rho):
+        rho = np.ascontiguousarray(rho, dtype=np.complex128)
+        if rho.size != self.offsets[-1]:
+            raise ValueError("packed state size mismatch")
+        self._call("quac_ensemble_set_states", rho.ctypes.data)
+
+    def get_states(self, out=None):
+        if out is None:
+            out = np.empty(self.offsets[-1], dtype=np.complex128)
+        self._call("quac_ensemble_get_states", out.ctypes.data)
+        return out
+
+    def state(self, rho_packed, i):
+        """Instance i's D x D density matrix out of a packed state array."""
+        D = int(self.dims[i])
+        return rho_packed[self.offsets[i]:self.offsets[i + 1]].reshape(D, D, order="F")
+
+    def device_ptr(self):
+        return lib().quac_ensemble_state_device_ptr(self._h)
+
+    def run(self, t0, tmax, dt0):
+        self._call("quac_ensemble_run", t0, tmax, dt0)
+
+    def stats(self):
+        t, st, rj, fl = dbl(), i64(), i64(), ctypes.c_int()
+        out = np.zeros((self.n, 4))
+        for i in range(self.n):
+            self._call("quac_ensemble_get_stats", i, ctypes.byref(t), ctypes.byref(st), ctypes.byref(rj),
+                       ctypes.byref(fl))
+            out[i] = (t.value, st.value, rj.value, fl.value)
+        return out
+
+    def populations(self, out=None):
+        if out is None:
+            out = np.empty(int(self.dims.sum()), dtype=np.float64)
+        self._call("quac_ensemble_populations", out.ctypes.data)
+        return out
+
+    def destroy(self):
+        if self._h:
+            lib().quac_ensemble_destroy(self._h)
+            self._h = None

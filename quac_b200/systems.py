@@ -95,3 +95,25 @@ def tavis_cummings(S, ne=6, nc=8, omega=0.3, delta=0.5, kappa=0.1, gamma=5e-3, g
     for e in ems:
         S.lin(gamma, e.a)
     return ems, cav
+
+
+def driven_jc_ensemble_params(count, seed=11, nc_lo=5, nc_hi=40):
+    """Parameter draws of the driven Jaynes-Cummings ensemble: cavity
+    truncation nc ~ U{nc_lo..nc_hi}, detuning ~ U[-0.5, 0.5], g ~ U[0.01, 0.2],
+    drive omega ~ U[0, 0.3], kappa log-uniform on [1e-3, 1e-1], gamma = 1e-3."""
+    rng = np.random.default_rng(seed)
+    nc = rng.integers(nc_lo, nc_hi + 1, size=count)
+    delta = rng.uniform(-0.5, 0.5, size=count)
+    g = rng.uniform(0.01, 0.2, size=count)
+    omega = rng.uniform(0.0, 0.3, size=count)
+    kappa = 10.0 ** rng.uniform(-3.0, -1.0, size=count)
+    return [dict(nc=int(nc[i]), delta=float(delta[i]), g=float(g[i]), omega=float(omega[i]),
+                 kappa=float(kappa[i])) for i in range(count)]
+
+
+def excited_vacuum(nc):
+    """rho0 = |e><e| (x) |0><0| of a driven JC system (emitter first), column-stacked."""
+    D = 2 * nc
+    rho = np.zeros(D * D, dtype=np.complex128)
+    rho[nc * D + nc] = 1.0
+    return rho

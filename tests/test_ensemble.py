@@ -1,0 +1,128 @@
+"""Batched ensemble integration against the oracle, instance by instance.
+
+Each instance is a driven Jaynes-Cummings system with its own cavity
+truncation; the oracle integrates each one alone with the same
+Dormand-Prince 5(4) controller (oracle.dp5).  FP64 mode must agree to
+1e-10 relative (same arithmetic up to summation order); the FP32
+right-hand-side mode is held to the population bar stated in each test.
+"""
+import numpy as np
+import pytest
+
+from quac_b200 import systems as Sy
+
+pytestmark = pytest.mark.gpu
+
+T_END, DT0 = 5.0, 0.05
+
+
+def _ensemble(q, params):
+    built = []
+    for p in params:
+        B = Sy.Builder(q)
+        Sy.driven_jc(B, **p)
+        built.append(B.qs)
+    E = q.Ensemble(built)
+    for qs in built:
+        qs.destroy()
+    rho0 = np.concatenate([Sy.excited_vacuum(p["nc"]) for p in params])
+    return E, rho0
+
+
+def _oracle_states(oracle, params, tmax, **kw):
+    out = []
+    for p in params:
+        O = oracle.OSys()
+        Sy.driven_jc(O, **p)
+        h = O.csr_handle()
+        y, nacc, nrej = oracle.dp5(h, Sy.excited_vacuum(p["nc"]), 0.0, tmax, DT0, **kw)
+        oracle.free_csr(h)
+        out.append((y, nacc, nrej))
+    return out
+
+
+# mixed sizes: small instances run one per warp, the largest take a whole CTA
+PARAMS = Sy.driven_jc_ensemble_params(20, seed=5, nc_lo=3, nc_hi=40)
+
+
+@pytest.fixture(scope="module")
+def reference(oracle):
+    return _oracle_states(oracle, PARAMS, T_END)
+
+
+def test_ensemble_fp64_matches_oracle(quac, reference):
+    E, rho0 = _ensemble(quac, PARAMS)
+    E.set_states(rho0)
+    E.run(0.0, T_END, DT0)
+    y = E.get_states()
+    st = E.stats()
+    for i, (yo, nacc, nrej) in enumerate(reference):
+        yi = y[E.offsets[i]:E.offsets[i + 1]]
+        assert np.linalg.norm(yi - yo) / np.linalg.norm(yo) < 1e-10, i
+        assert st[i, 0] == pytest.approx(T_END)
+        assert (st[i, 1], st[i, 2]) == (nacc, nrej)
+    E.destroy()
+
+
+@pytest.mark.parametrize("shape", [(8, 1, 2), (16, 1, 8), (32, 1, 16), (16, 1, 4), (4, 1, 32)])
+def test_ensemble_launch_shapes_agree(quac, reference, shape):
+    E, rho0 = _ensemble(quac, PARAMS)
+    E.set_shape(*shape)
+    E.set_states(rho0)
+    E.run(0.0, T_END, DT0)
+    y = E.get_states()
+    for i, (yo, _, _) in enumerate(reference):
+        yi = y[E.offsets[i]:E.offsets[i + 1]]
+        assert np.linalg.norm(yi - yo) / np.linalg.norm(yo) < 1e-10, (shape, i)
+    E.destroy()
+
+
+def test_ensemble_rerun_is_deterministic_and_tune_keeps_states(quac):
+    E, rho0 = _ensemble(quac, PARAMS)
+    E.set_states(rho0)
+    E.tune(0.0, 0.5, DT0)
+    assert np.array_equal(E.get_states(), rho0)
+    E.run(0.0, 1.0, DT0)
+    a = E.get_states()
+    E.set_states(rho0)
+    E.run(0.0, 1.0, DT0)
+    b = E.get_states()
+    assert np.array_equal(a, b)
+    # populations read back by the device kernel equal the diagonal
+    pops = E.populations()
+    k = 0
+    for i, D in enumerate(E.dims):
+        rho = a[E.offsets[i]:E.offsets[i + 1]].reshape(D, D, order="F")
+        assert np.array_equal(pops[k:k + D], rho.diagonal().real)
+        k += D
+    E.destroy()
+
+
+def test_ensemble_fp32_rhs_population_error(quac, reference):
+    E, rho0 = _ensemble(quac, PARAMS)
+    E.set_options(precision=1)
+    E.set_states(rho0)
+    E.run(0.0, T_END, DT0)
+    y = E.get_states()
+    worst = worst_tr = 0.0
+    for i, (yo, _, _) in enumerate(reference):
+        D = E.dims[i]
+        yi = y[E.offsets[i]:E.offsets[i + 1]].reshape(D, D, order="F")
+        ro = yo.reshape(D, D, order="F")
+        worst = max(worst, np.abs(yi.diagonal().real - ro.diagonal().real).max())
+        worst_tr = max(worst_tr, abs(np.trace(yi) - 1.0))
+    print(f"fp32-rhs worst population error {worst:.3e}, trace error {worst_tr:.3e}")
+    # complex64 increments: the error grows like eps32 * (variation of rho along the run)
+    assert worst < 1e-7 and worst_tr < 1e-7
+    E.destroy()
+
+
+def test_ensemble_rejects_bad_input(quac):
+    E, rho0 = _ensemble(quac, PARAMS[:2])
+    with pytest.raises(quac.QuacError):
+        E.set_options(precision=3)
+    with pytest.raises(quac.QuacError):
+        E.set_shape(12, 1, 8)
+    with pytest.raises(quac.QuacError):
+        E.run(1.0, 0.0, DT0)
+    E.destroy()

@@ -300,6 +300,16 @@ int quac_ensemble_get_stats(quac_ensemble ens, int64_t i, double *t, int64_t *st
                             int *flags);
 /* Re(diag rho_i) of every instance, packed: D_0 values, then D_1, ... */
 int quac_ensemble_populations(quac_ensemble ens, double *pops);
+/* Steady state from a proposed initial state and a proposed dominant
+ * subspace (no reference counterpart; solver.c:33-221 always starts from
+ * e0).  x holds the initial guess on entry.  U: D x kd column-major, with
+ * orthonormal columns (kd <= 8); the kd^2 matrices u_i u_j^H span the
+ * deflation space of the preconditioner.  Deflated GMRES(100) runs for at
+ * most maxit_guided iterations, then plain GMRES(100) continues from its
+ * iterate if needed.  Same system and tolerance as steady_state.  Returns
+ * the iterations (-1 on error); *residual = ||b - A x|| at the end. */
+PetscInt quac_steady_state_guided(qsystem qsys, qvec x, const PetscScalar *U, PetscInt kd,
+                                  PetscInt maxit_guided, PetscReal *residual);
 /* Time-steps host data in place: one call = H2D + integration + D2H. */
 int quac_time_step_host(qsystem qsys, PetscScalar *x_host, PetscReal t0, PetscReal tmax,
                         PetscReal dt, PetscInt steps_max);

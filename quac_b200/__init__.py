@@ -168,6 +168,7 @@ def lib():
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "read_qvec_wf_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "print_qvec_file": (None, [P(_QvecStruct), ctypes.c_char_p]),
+        "quac_steady_state_guided": (i64, [P(_QsysStruct), P(_QvecStruct), vp, i64, i64, P(dbl)]),
         "quac_ensemble_create": (ctypes.c_int, [P(vp), i64, P(P(_QsysStruct))]),
         "quac_ensemble_destroy": (ctypes.c_int, [vp]),
         "quac_ensemble_set_options": (ctypes.c_int, [vp, ctypes.c_int, dbl, dbl, dbl, dbl, i64]),
@@ -606,6 +607,21 @@ def steady_state_sys(qs, q):
     its = lib().steady_state_sys(qs._ptr, q._ptr)
     _check()
     return its
+
+
+def steady_state_guided(qs, q, U=None, maxit_guided=20000):
+    """Steady state from the initial guess already in q, deflated by the
+    dominant subspace U (D x kd, orthonormal columns).  Returns (iterations,
+    final residual ||b - A x||)."""
+    res = dbl()
+    if U is None:
+        its = lib().quac_steady_state_guided(qs._ptr, q._ptr, None, 0, maxit_guided, ctypes.byref(res))
+    else:
+        U = np.asfortranarray(U, dtype=np.complex128)
+        its = lib().quac_steady_state_guided(qs._ptr, q._ptr, U.ctypes.data, U.shape[1], maxit_guided,
+                                             ctypes.byref(res))
+    _check()
+    return its, res.value
 
 
 def lrho_apply_device(qs, x_ptr, y_ptr):

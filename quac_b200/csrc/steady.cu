@@ -137,6 +137,126 @@ __global__ void k_e0_minus(double2 *__restrict__ r, int64_t n) {
   }
 }
 
+// ---- deflation by a proposed dominant subspace U (D x kd, orthonormal) ----
+// W = { vec(u_i u_j^H) } (kd^2 orthonormal vectors); W^H x = U^H X U.
+constexpr int DR = 128;  // rows per block
+constexpr int DC = 32;   // columns per block
+constexpr int KDMAX = 8;
+
+// partial[b][i*kd + j] = sum over this block's rows r and columns c of conj(U[r,i]) X[r,c] U[c,j]
+__global__ void k_defl_proj(const double2 *__restrict__ X, const double2 *__restrict__ U, int D, int kd,
+                            double2 *__restrict__ partial) {
+  __shared__ double2 Uc[DC][KDMAX];
+  __shared__ double2 red[DR / 32][KDMAX * KDMAX];
+  const int r = blockIdx.x * DR + threadIdx.x, c0 = blockIdx.y * DC;
+  for (int q = threadIdx.x; q < DC * kd; q += DR) {
+    const int cc = q / kd, j = q % kd;
+    Uc[cc][j] = (c0 + cc < D) ? U[(size_t)j * D + c0 + cc] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  double2 T[KDMAX];
+  for (int j = 0; j < KDMAX; j++) T[j] = make_double2(0.0, 0.0);
+  if (r < D) {
+    for (int cc = 0; cc < DC && c0 + cc < D; cc++) {
+      const double2 x = X[(size_t)(c0 + cc) * D + r];
+      for (int j = 0; j < kd; j++) {
+        const double2 u = Uc[cc][j];
+        T[j].x = fma(x.x, u.x, fma(-x.y, u.y, T[j].x));
+        T[j].y = fma(x.x, u.y, fma(x.y, u.x, T[j].y));
+      }
+    }
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = 0; i < kd; i++) {
+    double2 ui = (r < D) ? U[(size_t)i * D + r] : make_double2(0.0, 0.0);
+    ui.y = -ui.y;
+    for (int j = 0; j < kd; j++) {
+      double2 p = cmuls(ui, T[j]);
+      for (int o = 16; o > 0; o >>= 1) {
+        p.x += __shfl_down_sync(0xffffffffu, p.x, o);
+        p.y += __shfl_down_sync(0xffffffffu, p.y, o);
+      }
+      if (lane == 0) red[w][i * kd + j] = p;
+    }
+  }
+  __syncthreads();
+  const int b = blockIdx.y * gridDim.x + blockIdx.x;
+  for (int q = threadIdx.x; q < kd * kd; q += DR) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int ww = 0; ww < DR / 32; ww++) { acc.x += red[ww][q].x; acc.y += red[ww][q].y; }
+    partial[(size_t)b * kd * kd + q] = acc;
+  }
+}
+
+// z = sum_b partial[b]; c = Cm z (Cm = E^-1 - I, kd^2 x kd^2 row-major); then
+// P = U C with C[i][j] = c[i*kd + j]  (D x kd)
+__global__ void k_defl_coef(const double2 *__restrict__ partial, int nb, const double2 *__restrict__ Cm,
+                            int kd, double2 *__restrict__ zc, int mode) {
+  __shared__ double2 z[KDMAX * KDMAX];
+  const int K2 = kd * kd;
+  for (int q = threadIdx.x; q < K2; q += blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int b = 0; b < nb; b++) { acc.x += partial[(size_t)b * K2 + q].x; acc.y += partial[(size_t)b * K2 + q].y; }
+    z[q] = acc;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < K2; q += blockDim.x) {
+    if (mode == 0) {  // projections only
+      zc[q] = z[q];
+    } else {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int p = 0; p < K2; p++) {
+        const double2 t = cmuls(Cm[(size_t)q * K2 + p], z[p]);
+        acc.x += t.x; acc.y += t.y;
+      }
+      zc[q] = acc;
+    }
+  }
+}
+
+// out[r,c] = in[r,c] + sum_{i,j} U[r,i] C[i,j] conj(U[c,j])
+__global__ void k_defl_expand(const double2 *__restrict__ in, double2 *__restrict__ out,
+                              const double2 *__restrict__ U, const double2 *__restrict__ cvec, int D, int kd) {
+  __shared__ double2 C[KDMAX * KDMAX];
+  __shared__ double2 Uc[DC][KDMAX];
+  const int r = blockIdx.x * DR + threadIdx.x, c0 = blockIdx.y * DC;
+  for (int q = threadIdx.x; q < kd * kd; q += DR) C[q] = cvec[q];
+  for (int q = threadIdx.x; q < DC * kd; q += DR) {
+    const int cc = q / kd, j = q % kd;
+    double2 u = (c0 + cc < D) ? U[(size_t)j * D + c0 + cc] : make_double2(0.0, 0.0);
+    u.y = -u.y;
+    Uc[cc][j] = u;
+  }
+  __syncthreads();
+  if (r >= D) return;
+  double2 P[KDMAX];
+  for (int j = 0; j < kd; j++) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int i = 0; i < kd; i++) {
+      const double2 t = cmuls(U[(size_t)i * D + r], C[i * kd + j]);
+      acc.x += t.x; acc.y += t.y;
+    }
+    P[j] = acc;
+  }
+  for (int cc = 0; cc < DC && c0 + cc < D; cc++) {
+    const size_t e = (size_t)(c0 + cc) * D + r;
+    double2 v = in[e];
+    for (int j = 0; j < kd; j++) {
+      const double2 t = cmuls(P[j], Uc[cc][j]);
+      v.x += t.x; v.y += t.y;
+    }
+    out[e] = v;
+  }
+}
+
+// y = x + a * y  (a real)
+__global__ void k_axpy_inplace(double2 *__restrict__ y, const double2 *__restrict__ x, int64_t n, double a) {
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    const double2 v = x[i], w = y[i];
+    y[i] = make_double2(w.x + a * v.x, w.y + a * v.y);
+  }
+}
+
 int grid_for(int64_t n) {
   int64_t b = (n + NT - 1) / NT;
   return (int)std::min<int64_t>(b, 148 * 8);
@@ -193,9 +313,110 @@ static double norm2(const double2 *x, int64_t n, cudaStream_t s) {
   return std::sqrt(std::max(0.0, vdot(x, x, n, s).real()));
 }
 
+// Deflation preconditioner M = I + W (E^-1 - I) W^H with W = { vec(u_i u_j^H) }
+// and E = W^H A W (kd^2 x kd^2): the components of the residual in span W are
+// solved for exactly, so restarted GMRES no longer stalls on the slow modes
+// that W captures.
+struct Deflation {
+  int D = 0, kd = 0, nbx = 0, nby = 0;
+  double2 *U = nullptr, *Cm = nullptr, *partial = nullptr, *coef = nullptr, *t1 = nullptr, *t2 = nullptr;
+  void release() {
+    for (double2 *p : {U, Cm, partial, coef, t1, t2})
+      if (p) cudaFree(p);
+    U = Cm = partial = coef = t1 = t2 = nullptr;
+  }
+};
+
+static void defl_project(const Deflation &F, const double2 *in, const double2 *Cm, double2 *coef, int mode,
+                         cudaStream_t s) {
+  dim3 g(F.nbx, F.nby);
+  k_defl_proj<<<g, DR, 0, s>>>(in, F.U, F.D, F.kd, F.partial);
+  k_defl_coef<<<1, 128, 0, s>>>(F.partial, F.nbx * F.nby, Cm, F.kd, coef, mode);
+  count_launch(2);
+}
+
+// out = M in
+static void apply_M(const Deflation &F, const double2 *in, double2 *out, cudaStream_t s) {
+  defl_project(F, in, F.Cm, F.coef, 1, s);
+  k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(in, out, F.U, F.coef, F.D, F.kd);
+  count_launch();
+}
+
+// Inverse of a small dense complex matrix (row-major, Gauss-Jordan with partial pivoting).
+static bool invert_small(std::vector<std::complex<double>> &A, int n) {
+  std::vector<std::complex<double>> I((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) I[(size_t)i * n + i] = 1.0;
+  for (int c = 0; c < n; c++) {
+    int piv = c;
+    for (int r = c + 1; r < n; r++)
+      if (std::abs(A[(size_t)r * n + c]) > std::abs(A[(size_t)piv * n + c])) piv = r;
+    if (std::abs(A[(size_t)piv * n + c]) < 1e-300) return false;
+    if (piv != c)
+      for (int k = 0; k < n; k++) {
+        std::swap(A[(size_t)c * n + k], A[(size_t)piv * n + k]);
+        std::swap(I[(size_t)c * n + k], I[(size_t)piv * n + k]);
+      }
+    const std::complex<double> d = 1.0 / A[(size_t)c * n + c];
+    for (int k = 0; k < n; k++) { A[(size_t)c * n + k] *= d; I[(size_t)c * n + k] *= d; }
+    for (int r = 0; r < n; r++) {
+      if (r == c) continue;
+      const std::complex<double> f = A[(size_t)r * n + c];
+      if (f == 0.0) continue;
+      for (int k = 0; k < n; k++) { A[(size_t)r * n + k] -= f * A[(size_t)c * n + k]; I[(size_t)r * n + k] -= f * I[(size_t)c * n + k]; }
+    }
+  }
+  A.swap(I);
+  return true;
+}
+
+// Builds the deflation preconditioner from host U (D x kd, column-major).
+static bool build_deflation(const DeviceProgram &PP, const std::complex<double> *U_host, int kd, Deflation &F,
+                            cudaStream_t s) {
+  const int D = PP.dev.D;
+  const int64_t n = (int64_t)D * D;
+  F.D = D;
+  F.kd = kd;
+  F.nbx = (D + DR - 1) / DR;
+  F.nby = (D + DC - 1) / DC;
+  const int K2 = kd * kd;
+  QCUDA(cudaMalloc(&F.U, (size_t)D * kd * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.Cm, (size_t)K2 * K2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.partial, (size_t)F.nbx * F.nby * K2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.coef, (size_t)K2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.t1, n * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.t2, n * sizeof(double2)));
+  if (has_error()) return false;
+  QCUDA(cudaMemcpyAsync(F.U, U_host, (size_t)D * kd * sizeof(double2), cudaMemcpyHostToDevice, s));
+  // E[:, (k,l)] = W^H A vec(u_k u_l^H)
+  std::vector<std::complex<double>> E((size_t)K2 * K2);
+  std::vector<double2> unit(K2), col(K2);
+  for (int q = 0; q < K2; q++) {
+    for (int p = 0; p < K2; p++) unit[p] = make_double2(p == q ? 1.0 : 0.0, 0.0);
+    QCUDA(cudaMemcpyAsync(F.coef, unit.data(), K2 * sizeof(double2), cudaMemcpyHostToDevice, s));
+    QCUDA(cudaMemsetAsync(F.t1, 0, n * sizeof(double2), s));
+    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(F.t1, F.t1, F.U, F.coef, D, kd);
+    count_launch();
+    apply_A(PP, F.t1, F.t2, s);
+    defl_project(F, F.t2, nullptr, F.coef, 0, s);
+    QCUDA(cudaMemcpyAsync(col.data(), F.coef, K2 * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    QCUDA(cudaStreamSynchronize(s));
+    for (int p = 0; p < K2; p++) E[(size_t)p * K2 + q] = std::complex<double>(col[p].x, col[p].y);
+  }
+  if (has_error() || !invert_small(E, K2)) return false;
+  std::vector<double2> Cm((size_t)K2 * K2);
+  for (int p = 0; p < K2; p++)
+    for (int q = 0; q < K2; q++) {
+      std::complex<double> v = E[(size_t)p * K2 + q] - (p == q ? 1.0 : 0.0);
+      Cm[(size_t)p * K2 + q] = make_double2(v.real(), v.imag());
+    }
+  QCUDA(cudaMemcpyAsync(F.Cm, Cm.data(), Cm.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+  QCUDA(cudaStreamSynchronize(s));
+  return !has_error();
+}
+
 // Returns iterations, fills x (device, length n).  rtol is relative to ||b|| = 1.
 int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, bool x_is_guess,
-                    double *final_res) {
+                    double *final_res, const Deflation *def = nullptr) {
   ensure_program(qs);
   const DeviceProgram &PP = *qs->impl->prog;
   const DevProg &P = PP.dev;
@@ -227,7 +448,12 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
     int j = 0;
     bool conv = false;
     for (; j < m && it < maxit; j++, it++) {
-      apply_A(PP, G.V + (size_t)j * n, G.w, s);
+      if (def) {  // right preconditioning: Arnoldi on A M
+        apply_M(*def, G.V + (size_t)j * n, def->t1, s);
+        apply_A(PP, def->t1, G.w, s);
+      } else {
+        apply_A(PP, G.V + (size_t)j * n, G.w, s);
+      }
       // CGS2 with the projections summed on the host
       std::vector<std::complex<double>> hsum(j + 1, 0.0);
       for (int pass = 0; pass < 2; pass++) {
@@ -271,8 +497,16 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
       std::vector<double2> yh(j);
       for (int k = 0; k < j; k++) yh[k] = make_double2(y[k].real(), y[k].imag());
       QCUDA(cudaMemcpyAsync(G.h, yh.data(), j * sizeof(double2), cudaMemcpyHostToDevice, s));
-      k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j, x, 1.0);
-      count_launch();
+      if (def) {  // x += M (V y)
+        QCUDA(cudaMemsetAsync(def->t1, 0, n * sizeof(double2), s));
+        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j, def->t1, 1.0);
+        apply_M(*def, def->t1, def->t2, s);
+        k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, def->t2, n, 1.0);
+        count_launch(2);
+      } else {
+        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j, x, 1.0);
+        count_launch();
+      }
       QCUDA(cudaStreamSynchronize(s));
     }
     (void)conv;
@@ -293,5 +527,39 @@ extern "C" PetscInt steady_state_sys(qsystem qs, qvec x) {
   vec_sync_to_device(x->data);
   double res = 0;
   const int64_t its = gmres_solve(qs, x->data->d, 1e-11, 100, 200000, false, &res);
+  return has_error() ? -1 : its;
+}
+
+// Steady state from a proposed initial state (x on entry) and a proposed
+// dominant subspace U (D x kd, orthonormal columns, column-major host array;
+// kd = 0: no deflation).  Deflated GMRES runs for at most maxit_guided
+// iterations; if it has not converged, plain GMRES(100) continues from its
+// iterate.  Returns the total number of iterations (-1 on error).
+extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScalar *U_host, PetscInt kd,
+                                             PetscInt maxit_guided, PetscReal *residual) {
+  if (!qs->dm_equations) { fail(0, "ERROR! steady state needs Lindblad terms\n"); return -1; }
+  if (kd < 0 || kd > KDMAX) { fail(0, "ERROR! deflation rank must be in [0, %d]\n", KDMAX); return -1; }
+  if (!qs->mat_allocated) construct_matrix(qs);
+  if (has_error()) return -1;
+  vec_sync_to_device(x->data);
+  ensure_program(qs);
+  const DeviceProgram &PP = *qs->impl->prog;
+  cudaStream_t s = stream_of(qs);
+  Deflation F;
+  const bool use = kd > 0;
+  if (use && !build_deflation(PP, reinterpret_cast<const std::complex<double> *>(U_host), (int)kd, F, s)) {
+    F.release();
+    return -1;
+  }
+  double res = 0;
+  int64_t its = gmres_solve(qs, x->data->d, 1e-11, 100, maxit_guided, true, &res, use ? &F : nullptr);
+  F.release();
+  if (its < 0) return -1;
+  if (res > 1e-11) {
+    const int64_t more = gmres_solve(qs, x->data->d, 1e-11, 100, 200000, true, &res);
+    if (more < 0) return -1;
+    its += more;
+  }
+  if (residual) *residual = res;
   return has_error() ? -1 : its;
 }

@@ -42,3 +42,73 @@ def test_gemm_tf32_matches_numpy(quac, M, N, K, act):
     bound = 3 * 2.0 ** -10 * (np.abs(A).astype(np.float64) @ np.abs(B).T.astype(np.float64)) + 1e-6
     assert np.all(np.abs(C - ref) <= bound)
     assert np.abs(C - ref).max() > 0  # really TF32 tensor-core arithmetic, not an FP32 fallback
+
+
+# ---------------------------------------------------------------- guided solve
+from quac_b200 import systems as Sy  # noqa: E402
+
+TC_POINT = dict(omega=0.403, delta=0.616, kappa=0.108, gamma=0.0036)
+
+
+def _oracle_steady(oracle, ne, nc, p):
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    O = oracle.OSys()
+    Sy.tavis_cummings(O, ne=ne, nc=nc, g=0.1, **p)
+    L = O.liouvillian().tocsr()
+    n = L.shape[0]
+    D = int(round(np.sqrt(n)))
+    row = sp.csr_matrix((np.eye(D).reshape(-1, order="F"), (np.zeros(n, int), np.arange(n))), shape=(n, n))
+    b = np.zeros(n, complex)
+    b[0] = 1
+    return spla.spsolve((L + row).tocsc(), b), D
+
+
+def _factors(x, D, r):
+    rho = x.reshape(D, D, order="F")
+    w, V = np.linalg.eigh((rho + rho.conj().T) / 2)
+    idx = np.argsort(-w)[:r]
+    return V[:, idx], w[idx]
+
+
+def test_guided_steady_state_with_exact_subspace(quac, oracle):
+    ne, nc = 3, 4
+    xs, D = _oracle_steady(oracle, ne, nc, TC_POINT)
+    B = Sy.Builder(quac)
+    Sy.tavis_cummings(B, ne=ne, nc=nc, g=0.1, **TC_POINT)
+    quac.construct_matrix(B.qs)
+    cold = quac.create_qvec_sys(B.qs)
+    its_cold = quac.steady_state_sys(B.qs, cold)
+    U, w = _factors(xs, D, 16)
+    x0 = (U * np.maximum(w, 0)) @ U.conj().T
+    x0 = (x0 / np.trace(x0)).reshape(-1, order="F")
+    g = quac.create_qvec_sys(B.qs)
+    g.from_numpy(x0)
+    its, res = quac.steady_state_guided(B.qs, g, U[:, :8])
+    y = g.to_numpy()
+    print(f"cold {its_cold} iterations, guided {its} iterations, residual {res:.2e}")
+    assert res <= 1e-11
+    assert 5 * its < its_cold
+    assert np.linalg.norm(y - xs) / np.linalg.norm(xs) < 1e-8
+    cold.destroy()
+    g.destroy()
+    B.qs.destroy()
+
+
+def test_guided_steady_state_falls_back_to_plain_gmres(quac, oracle):
+    ne, nc = 3, 4
+    xs, D = _oracle_steady(oracle, ne, nc, TC_POINT)
+    B = Sy.Builder(quac)
+    Sy.tavis_cummings(B, ne=ne, nc=nc, g=0.1, **TC_POINT)
+    quac.construct_matrix(B.qs)
+    rng = np.random.default_rng(1)
+    U, _ = np.linalg.qr(rng.normal(size=(D, 4)) + 1j * rng.normal(size=(D, 4)))
+    g = quac.create_qvec_sys(B.qs)
+    x0 = np.zeros(D * D, complex)
+    x0[0] = 1.0
+    g.from_numpy(x0)
+    its, res = quac.steady_state_guided(B.qs, g, U, maxit_guided=50)
+    assert res <= 1e-11 and its > 50
+    assert np.linalg.norm(g.to_numpy() - xs) / np.linalg.norm(xs) < 1e-8
+    g.destroy()
+    B.qs.destroy()

@@ -310,6 +310,24 @@ int quac_ensemble_populations(quac_ensemble ens, double *pops);
  * the iterations (-1 on error); *residual = ||b - A x|| at the end. */
 PetscInt quac_steady_state_guided(qsystem qsys, qvec x, const PetscScalar *U, PetscInt kd,
                                   PetscInt maxit_guided, PetscReal *residual);
+/* Learned warm start for steady states (no reference counterpart): an MLP
+ * (4 normalised parameters -> hidden -> hidden -> rank-r factors F, D x r
+ * complex) trained on steady states the solver produced; F F^H proposes
+ * the initial state and the leading directions of range F the deflation
+ * space of quac_steady_state_guided.  Dense layers run on the tensor cores
+ * (TF32, FP32 accumulation). */
+typedef struct quac_wsnet_s *quac_wsnet;
+int quac_wsnet_create(quac_wsnet *net, int D, int rank, int hidden, int batch, int max_samples, uint64_t seed);
+int quac_wsnet_destroy(quac_wsnet net);
+int quac_wsnet_add_sample(quac_wsnet net, const double *theta4, qvec rho);
+int quac_wsnet_num_samples(quac_wsnet net);
+int64_t quac_wsnet_num_params(quac_wsnet net);
+int quac_wsnet_get_params(quac_wsnet net, float *params);
+int quac_wsnet_set_params(quac_wsnet net, const float *params);
+/* Mean loss and its gradient over samples [0, nb), no update. */
+int quac_wsnet_loss_grad(quac_wsnet net, int nb, double *loss, float *grad);
+int quac_wsnet_train(quac_wsnet net, int epochs, double lr, uint64_t seed, double *final_loss);
+int quac_wsnet_predict(quac_wsnet net, int n, const double *theta4, PetscScalar *factors);
 /* Time-steps host data in place: one call = H2D + integration + D2H. */
 int quac_time_step_host(qsystem qsys, PetscScalar *x_host, PetscReal t0, PetscReal tmax,
                         PetscReal dt, PetscInt steps_max);

@@ -169,6 +169,17 @@ def lib():
         "read_qvec_wf_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "print_qvec_file": (None, [P(_QvecStruct), ctypes.c_char_p]),
         "quac_steady_state_guided": (i64, [P(_QsysStruct), P(_QvecStruct), vp, i64, i64, P(dbl)]),
+        "quac_wsnet_create": (ctypes.c_int, [P(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_uint64]),
+        "quac_wsnet_destroy": (ctypes.c_int, [vp]),
+        "quac_wsnet_add_sample": (ctypes.c_int, [vp, P(dbl), P(_QvecStruct)]),
+        "quac_wsnet_num_samples": (ctypes.c_int, [vp]),
+        "quac_wsnet_num_params": (i64, [vp]),
+        "quac_wsnet_get_params": (ctypes.c_int, [vp, vp]),
+        "quac_wsnet_set_params": (ctypes.c_int, [vp, vp]),
+        "quac_wsnet_loss_grad": (ctypes.c_int, [vp, ctypes.c_int, P(dbl), vp]),
+        "quac_wsnet_train": (ctypes.c_int, [vp, ctypes.c_int, dbl, ctypes.c_uint64, P(dbl)]),
+        "quac_wsnet_predict": (ctypes.c_int, [vp, ctypes.c_int, vp, vp]),
         "quac_ensemble_create": (ctypes.c_int, [P(vp), i64, P(P(_QsysStruct))]),
         "quac_ensemble_destroy": (ctypes.c_int, [vp]),
         "quac_ensemble_set_options": (ctypes.c_int, [vp, ctypes.c_int, dbl, dbl, dbl, dbl, i64]),
@@ -747,4 +758,70 @@ class Ensemble:
     def destroy(self):
         if self._h:
             lib().quac_ensemble_destroy(self._h)
+            self._h = None
+
+
+# ------------------------------------------------------- learned warm start
+class WarmStartNet:
+    """The steady-state warm-start network (quac_wsnet_*).
+
+    Inputs are 4 normalised parameters; the output for each input is a
+    D x rank complex factor matrix F with F F^H ~ rho_ss."""
+
+    def __init__(self, D, rank=16, hidden=256, batch=128, max_samples=2048, seed=0):
+        h = vp()
+        rc = lib().quac_wsnet_create(ctypes.byref(h), D, rank, hidden, batch, max_samples, seed)
+        _check()
+        if rc:
+            raise QuacError("quac_wsnet_create failed")
+        self._h, self.D, self.rank = h, D, rank
+
+    def _call(self, name, *args):
+        rc = getattr(lib(), name)(self._h, *args)
+        _check()
+        if rc:
+            raise QuacError(f"{name} failed")
+
+    def add_sample(self, theta, rho_qvec):
+        t = (dbl * 4)(*[float(v) for v in theta])
+        self._call("quac_wsnet_add_sample", t, rho_qvec._ptr)
+
+    @property
+    def num_samples(self):
+        return lib().quac_wsnet_num_samples(self._h)
+
+    @property
+    def num_params(self):
+        return lib().quac_wsnet_num_params(self._h)
+
+    def get_params(self):
+        out = np.empty(self.num_params, dtype=np.float32)
+        self._call("quac_wsnet_get_params", out.ctypes.data)
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.num_params
+        self._call("quac_wsnet_set_params", p.ctypes.data)
+
+    def loss_grad(self, nb):
+        loss = dbl()
+        g = np.empty(self.num_params, dtype=np.float32)
+        self._call("quac_wsnet_loss_grad", nb, ctypes.byref(loss), g.ctypes.data)
+        return loss.value, g
+
+    def train(self, epochs, lr=1e-3, seed=0):
+        loss = dbl()
+        self._call("quac_wsnet_train", epochs, lr, seed, ctypes.byref(loss))
+        return loss.value
+
+    def predict(self, thetas):
+        thetas = np.ascontiguousarray(np.atleast_2d(thetas), dtype=np.float64)
+        F = np.empty((thetas.shape[0], self.rank, self.D), dtype=np.complex128)
+        self._call("quac_wsnet_predict", thetas.shape[0], thetas.ctypes.data, F.ctypes.data)
+        return np.transpose(F, (0, 2, 1))  # (n, D, rank)
+
+    def destroy(self):
+        if self._h:
+            lib().quac_wsnet_destroy(self._h)
             self._h = None

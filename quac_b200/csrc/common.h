@@ -164,6 +164,9 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
 // Reads and clears the program's device error word; reports through fail().
 bool check_program_error(DeviceProgram &P, cudaStream_t s);
 void zero_epi(Epi &e);
+// C[M x N] = act(A[M x K] B[N x K]^T + bias), TF32 tensor cores; K % 32 == 0 (mlp.cu)
+void launch_gemm_tf32(const float *A, const float *B, float *C, const float *bias, int M, int N, int K, int act,
+                      int *err, cudaStream_t s);
 // lincomb.cu
 void launch_lincomb(double2 *out, const double2 *base, int nin, const double2 *const *in,
                     const double *coef, int64_t n, cudaStream_t s);

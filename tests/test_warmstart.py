@@ -112,3 +112,48 @@ def test_guided_steady_state_falls_back_to_plain_gmres(quac, oracle):
     assert np.linalg.norm(g.to_numpy() - xs) / np.linalg.norm(xs) < 1e-8
     g.destroy()
     B.qs.destroy()
+
+
+# ------------------------------------------------------------ network kernels
+def _random_states(rng, n, D):
+    out = []
+    for _ in range(n):
+        A = rng.normal(size=(D, 3)) + 1j * rng.normal(size=(D, 3))
+        rho = A @ A.conj().T
+        out.append(rho / np.trace(rho).real)
+    return np.array(out)
+
+
+def test_network_gradients_match_cpu_oracle(quac):
+    from oracle import wsnet_oracle as WO
+    D, r, H, n = 8, 4, 32, 6
+    rng = np.random.default_rng(3)
+    net = quac.WarmStartNet(D, rank=r, hidden=H, batch=8, max_samples=n, seed=11)
+    B = Sy.Builder(quac)
+    for _ in range(3):
+        B.op(2)
+    X = rng.uniform(-1, 1, size=(n, 4))
+    rhos = _random_states(rng, n, D)
+    for k in range(n):
+        v = quac.create_dm_sys(B.qs)
+        v.from_numpy(rhos[k].reshape(-1, order="F"))
+        net.add_sample(X[k], v)
+        v.destroy()
+    p = net.get_params()
+    # round the targets like the device copy (complex64)
+    rhos32 = rhos.astype(np.complex64).astype(np.complex128)
+    loss_ref, g_ref = WO.loss_grad(p, X.astype(np.float32).astype(np.float64), rhos32, D, r, H)
+    loss, g = net.loss_grad(n)
+    assert abs(loss - loss_ref) <= 1e-2 * loss_ref
+    W1, b1, W2, b2, W3, b3 = WO.unpack(np.arange(p.size), D, r, H)
+    for name, ix in zip(["W1", "b1", "W2", "b2", "W3", "b3"], [W1, b1, W2, b2, W3, b3]):
+        ix = np.asarray(ix).ravel().astype(int)
+        gr, gg = g_ref[ix], g[ix]
+        # TF32 operands (10-bit mantissa) in all six GEMMs of the pass
+        assert np.linalg.norm(gg - gr) <= 3e-2 * np.linalg.norm(gr) + 1e-7, name
+    # one Adam epoch lowers the loss on this batch
+    net.train(30, lr=1e-2, seed=1)
+    loss_after, _ = net.loss_grad(n)
+    assert loss_after < loss
+    net.destroy()
+    B.qs.destroy()

@@ -304,8 +304,9 @@ int quac_ensemble_populations(quac_ensemble ens, double *pops);
  * subspace (no reference counterpart; solver.c:33-221 always starts from
  * e0).  x holds the initial guess on entry.  U: D x kd column-major, with
  * orthonormal columns (kd <= 8); the kd^2 matrices u_i u_j^H span the
- * deflation space of the preconditioner.  Deflated GMRES(100) runs for at
- * most maxit_guided iterations, then plain GMRES(100) continues from its
+ * deflation space of the preconditioner.  The solve starts from x or e0,
+ * whichever has the smaller residual; deflated GMRES(100) runs for at most
+ * maxit_guided iterations, then plain GMRES(100) continues from its
  * iterate if needed.  Same system and tolerance as steady_state.  Returns
  * the iterations (-1 on error); *residual = ||b - A x|| at the end. */
 PetscInt quac_steady_state_guided(qsystem qsys, qvec x, const PetscScalar *U, PetscInt kd,

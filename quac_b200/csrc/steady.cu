@@ -551,6 +551,24 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
     F.release();
     return -1;
   }
+  // start from whichever of the proposal and e0 has the smaller residual
+  {
+    Gmres &G = gmres_for(qs);
+    const int64_t n = (int64_t)PP.dev.D * PP.dev.D;
+    G.ensure(n, 100);
+    apply_A(PP, x->data->d, G.w, s);
+    k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.w, n);
+    count_launch();
+    const double r_guess = norm2(G.w, n, s);
+    QCUDA(cudaMemsetAsync(G.V, 0, n * sizeof(double2), s));
+    const double2 one = make_double2(1.0, 0.0);
+    QCUDA(cudaMemcpyAsync(G.V, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
+    apply_A(PP, G.V, G.w, s);
+    k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.w, n);
+    count_launch();
+    const double r_e0 = norm2(G.w, n, s);
+    if (!(r_guess <= r_e0)) QCUDA(cudaMemcpyAsync(x->data->d, G.V, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  }
   double res = 0;
   int64_t its = gmres_solve(qs, x->data->d, 1e-11, 100, maxit_guided, true, &res, use ? &F : nullptr);
   F.release();

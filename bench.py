@@ -182,6 +182,70 @@ def run_reference(args, rank, world):
                 "reference algorithm timed instead"}))
 
 
+def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=4):
+    """Driven Jaynes-Cummings ensemble (4096 instances, n_c ~ U{5..40}, each
+    evolved to t = 100 with its own Dormand-Prince 5(4) step): solves/s of
+    the persistent batched kernel in FP64 and with complex64 right-hand-side
+    increments, against the plain path (time_step_sys, -ts_rk_type 5dp, one
+    system at a time) timed on a sample, and the population error of the
+    FP32-increment mode against the FP64 ensemble (which the parity tests
+    hold to the oracle at 1e-10)."""
+    from quac_b200 import systems as Sy
+    params = Sy.driven_jc_ensemble_params(n_inst)
+    built = []
+    for p in params:
+        B = Sy.Builder(q)
+        Sy.driven_jc(B, **p)
+        built.append(B.qs)
+    E = q.Ensemble(built)
+    for qs in built:
+        qs.destroy()
+    rho0 = np.concatenate([Sy.excited_vacuum(p["nc"]) for p in params])
+    out = {"workload": f"driven_jc_ensemble_{n_inst}", "t_end": tmax, "controller": "DP5(4) atol=rtol=5e-7"}
+    states = {}
+    for mode, name in ((0, "fp64"), (1, "fp32_rhs")):
+        E.set_options(precision=mode)
+        E.set_states(rho0)
+        E.run(0.0, 0.5, dt0)  # captures the graph
+        E.set_states(rho0)
+        t0 = time.perf_counter()
+        E.run(0.0, tmax, dt0)
+        dt = time.perf_counter() - t0
+        states[mode] = E.get_states()
+        st = E.stats()
+        out[name] = {"solves_per_s": n_inst / dt, "seconds": dt, "mean_steps": float(st[:, 1].mean()),
+                     "shape": list(E.shape())}
+    pops = lambda x, i: E.state(x, i).diagonal().real
+    err = np.array([np.abs(pops(states[0], i) - pops(states[1], i)).max() for i in range(n_inst)])
+    out["fp32_rhs"]["pop_err_vs_fp64"] = {"median": float(np.median(err)), "p99": float(np.percentile(err, 99)),
+                                          "max": float(err.max()), "frac_le_1e-8": float((err <= 1e-8).mean())}
+    # plain path: one system at a time through time_step_sys
+    q.set_ts_options(rk_type="5dp", adapt_type="basic")
+    rng = np.random.default_rng(0)
+    tp, perr = 0.0, 0.0
+    for i in rng.choice(n_inst, size=plain_sample, replace=False):
+        p = params[i]
+        B = Sy.Builder(q)
+        Sy.driven_jc(B, **p)
+        q.construct_matrix(B.qs)
+        x = Sy.excited_vacuum(p["nc"])
+        t0 = time.perf_counter()
+        q.time_step_host(B.qs, x, 0.0, tmax, dt0, 10 ** 7)
+        tp += time.perf_counter() - t0
+        D = 2 * p["nc"]
+        perr = max(perr, float(np.abs(x.reshape(D, D, order="F").diagonal().real - pops(states[0], i)).max()))
+        B.qs.destroy()
+    q.set_ts_options(rk_type="3bs", adapt_type="basic")
+    plain = plain_sample / tp
+    out["plain_fp64_solves_per_s"] = plain
+    out["plain_sample"] = plain_sample
+    out["fp64"]["vs_plain"] = out["fp64"]["solves_per_s"] / plain
+    out["fp32_rhs"]["vs_plain"] = out["fp32_rhs"]["solves_per_s"] / plain
+    out["fp64"]["pop_err_vs_plain_max"] = perr
+    E.destroy()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import quac_b200 as q
@@ -274,6 +338,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        out["ensemble"] = ensemble_summary(q)
     q.set_ts_options(rk_type="3bs", adapt_type="basic")
     rho.destroy()
     qs.destroy()
@@ -287,6 +353,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

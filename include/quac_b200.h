@@ -353,6 +353,12 @@ void quac_set_stream(qsystem qsys, void *cuda_stream);
  * table kernel for every system, 2 = single-pass bit-mask kernel whenever
  * the system is all-qubit. */
 void quac_set_kernel_path(int path);
+/* Contraction precision of L.x (no reference counterpart): 0 = complex128
+ * (default), 1 = complex64 contraction and accumulation inside the
+ * multi-pass bit-mask kernel (all-qubit systems of seven or more qubits),
+ * with the state, the RK stage combinations, the error norm and every
+ * reduction kept in complex128.  Other kernels always run complex128. */
+int quac_set_lrho_precision(int precision);
 /* Number of kernels this library has launched (diagnostics). */
 int64_t quac_kernel_launch_count(void);
 

@@ -164,6 +164,7 @@ def lib():
         "quac_kernel_launch_count": (i64, []),
         "quac_set_stream": (None, [P(_QsysStruct), vp]),
         "quac_set_kernel_path": (None, [ctypes.c_int]),
+        "quac_set_lrho_precision": (ctypes.c_int, [ctypes.c_int]),
         "VecGetSize": (ctypes.c_int, [vp, P(i64)]),
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "read_qvec_wf_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
@@ -670,6 +671,12 @@ def set_stream(qs, stream_ptr):
 def set_kernel_path(path):
     """0: default selection; 1: generic table kernel; 2: single-pass bit-mask kernel."""
     lib().quac_set_kernel_path(int(path))
+
+
+def set_lrho_precision(precision):
+    """0: complex128 L.x; 1: complex64 contraction in the multi-pass kernel."""
+    lib().quac_set_lrho_precision(int(precision))
+    _check()
 
 
 # ---------------------------------------------------------------- ensembles

@@ -1180,3 +1180,9 @@ extern "C" void quac_set_stream(qsystem qs, void *stream) {
 extern "C" void quac_set_kernel_path(int path) {
   options().kernel_path = path;
 }
+
+extern "C" int quac_set_lrho_precision(int precision) {
+  if (precision != 0 && precision != 1) { fail(0, "ERROR! L.rho precision must be 0 (FP64) or 1 (FP32 contraction)\n"); return 1; }
+  options().lrho_f32 = precision;
+  return 0;
+}

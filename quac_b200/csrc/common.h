@@ -160,7 +160,8 @@ void launch_lrho_any(const DeviceProgram &P, const double2 *x, const Epi &e, cud
 bool compile_qubit(qsystem qs, const HostProg &hp, DeviceProgram *P);
 bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out);
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
-                         const Epi &e, cudaStream_t s);
+                         const Epi &e, cudaStream_t s,
+                         bool f32 = false);
 // Reads and clears the program's device error word; reports through fail().
 bool check_program_error(DeviceProgram &P, cudaStream_t s);
 void zero_epi(Epi &e);

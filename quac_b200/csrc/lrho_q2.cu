@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <array>
 #include <cstring>
+#include <type_traits>
 
 #include <cuda.h>
 
@@ -34,6 +35,18 @@ __device__ __forceinline__ void cfma2(double2 &acc, double2 a, double2 b) {
   acc.y = fma(a.x, b.y, acc.y);
   acc.y = fma(a.y, b.x, acc.y);
 }
+__device__ __forceinline__ void cfma2(float2 &acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(-a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(a.y, b.x, acc.y);
+}
+template <typename V2>
+__device__ __forceinline__ V2 to_v2(double2 v);
+template <>
+__device__ __forceinline__ double2 to_v2<double2>(double2 v) { return v; }
+template <>
+__device__ __forceinline__ float2 to_v2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
 __device__ __forceinline__ double2 cmul2(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
@@ -130,7 +143,7 @@ __device__ __forceinline__ void tma_tile(const PassParams &P, const CUtensorMap 
 // compile-time mask of the canonical single-bit kinds present: 1 = left X,
 // 2 = right X, 4 = lowering jump, 8 = raising jump; CANON < 0 means the
 // kinds are decided at run time.
-template <bool REAL, bool TMA, int NTHR, int CANON>
+template <bool REAL, bool TMA, int NTHR, int CANON, bool F32>
 __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassParams P,
                                                    const __grid_constant__ CUtensorMap tmap,
                                                    const double2 *__restrict__ X, const Epi E) {
@@ -138,6 +151,10 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
   constexpr int NW = NTHR / 32;
   constexpr int MC = 64 / NW;
   constexpr int NST = TMA ? 3 : 2;   // pipeline stages
+  // complex128 contraction, or (F32) complex64 contraction of tiles
+  // converted in shared memory, accumulated in complex64
+  using V2 = typename std::conditional<F32, float2, double2>::type;
+  using S = typename std::conditional<F32, float, double>::type;
   extern __shared__ __align__(128) double2 sm[];
   double2 *gts = sm + NST * NEL;     // ngroups * 64, layout [g][col bits][row bits]
   __shared__ double red[PT / 32];
@@ -191,6 +208,20 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
       cp_wait<1>();
       __syncthreads();
     }
+    const V2 *tile = reinterpret_cast<const V2 *>(cur);
+    if (F32) {
+      // in place: every thread reads its complex128 elements before any
+      // complex64 value is written over them
+      double2 tmp[NEL / PT];
+#pragma unroll
+      for (int k2 = 0; k2 < NEL / PT; k2++) tmp[k2] = cur[threadIdx.x + k2 * PT];
+      __syncthreads();
+      float2 *c32 = reinterpret_cast<float2 *>(cur);
+#pragma unroll
+      for (int k2 = 0; k2 < NEL / PT; k2++)
+        c32[threadIdx.x + k2 * PT] = make_float2((float)tmp[k2].x, (float)tmp[k2].y);
+      __syncthreads();
+    }
     unsigned rfix, cfix;
     tile_origin(t, n, lo, rfix, cfix);
     unsigned rl[2] = {(unsigned)lane, (unsigned)lane + 32u};
@@ -202,17 +233,18 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
     for (int i = 0; i < 2; i++) r[i] = rfix | (rl[i] << lo);
 #pragma unroll
     for (int m = 0; m < MC; m++) c[m] = cfix | (cl[m] << lo);
-    double2 acc[2][MC];
+    V2 acc[2][MC];
     if (P.accin) {
+      const V2 *ain = reinterpret_cast<const V2 *>(P.accin);
 #pragma unroll
       for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int m = 0; m < MC; m++) acc[i][m] = P.accin[(size_t)c[m] * D + r[i]];
+        for (int m = 0; m < MC; m++) acc[i][m] = ain[(size_t)c[m] * D + r[i]];
     } else {
 #pragma unroll
       for (int i = 0; i < 2; i++)
 #pragma unroll
-        for (int m = 0; m < MC; m++) acc[i][m] = make_double2(0.0, 0.0);
+        for (int m = 0; m < MC; m++) acc[i][m] = to_v2<V2>(make_double2(0.0, 0.0));
     }
     if (P.diag) {
       // groups 0 and 1 vary inside the tile (lo == 0 here); the others are
@@ -241,7 +273,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
             d.x += v1.x;
             d.y += v1.y;
           }
-          cfma2(acc[i][m], d, cur[cl[m] * 64 + rl[i]]);
+          cfma2(acc[i][m], to_v2<V2>(d), tile[cl[m] * 64 + rl[i]]);
         }
       }
     }
@@ -255,36 +287,36 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
       for (int b = 0; b < 6; b++) {
         const unsigned f = 1u << b;
         if (C_HL) {
-          const double hl = P.hl[b];
+          const S hl = (S)P.hl[b];
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
             for (int m = 0; m < MC; m++) {
-              const double2 p = cur[cl[m] * 64 + (rl[i] ^ f)];
+              const V2 p = tile[cl[m] * 64 + (rl[i] ^ f)];
               acc[i][m].x = fma(-hl, p.y, acc[i][m].x);
               acc[i][m].y = fma(hl, p.x, acc[i][m].y);
             }
         }
         if (C_HR) {
-          const double hr = P.hr[b];
+          const S hr = (S)P.hr[b];
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
             for (int m = 0; m < MC; m++) {
-              const double2 p = cur[(cl[m] ^ f) * 64 + rl[i]];
+              const V2 p = tile[(cl[m] ^ f) * 64 + rl[i]];
               acc[i][m].x = fma(-hr, p.y, acc[i][m].x);
               acc[i][m].y = fma(hr, p.x, acc[i][m].y);
             }
         }
         if (C_GL || C_GU) {
-          const double gl = C_GL ? P.gl[b] : 0.0, gu = C_GU ? P.gu[b] : 0.0;
+          const S gl = C_GL ? (S)P.gl[b] : (S)0, gu = C_GU ? (S)P.gu[b] : (S)0;
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
             for (int m = 0; m < MC; m++) {
               const bool rb = rl[i] & f, cb = cl[m] & f;
-              const double g = (rb != cb) ? 0.0 : (rb ? gu : gl);
-              const double2 p = cur[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
+              const S g = (rb != cb) ? (S)0 : (rb ? gu : gl);
+              const V2 p = tile[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
               acc[i][m].x = fma(g, p.x, acc[i][m].x);
               acc[i][m].y = fma(g, p.y, acc[i][m].y);
             }
@@ -300,17 +332,17 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         const bool neg = __popc(r[i] & T.smask) & 1;
         const unsigned pr = rl[i] ^ T.fl;
         if (REAL) {
-          const double wv = neg ? -T.coef.y : T.coef.y;
+          const S wv = (S)(neg ? -T.coef.y : T.coef.y);
 #pragma unroll
           for (int m = 0; m < MC; m++) {
-            const double2 p = cur[cl[m] * 64 + pr];
+            const V2 p = tile[cl[m] * 64 + pr];
             acc[i][m].x = fma(-wv, p.y, acc[i][m].x);
             acc[i][m].y = fma(wv, p.x, acc[i][m].y);
           }
         } else {
-          const double2 wv = neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef;
+          const V2 wv = to_v2<V2>(neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef);
 #pragma unroll
-          for (int m = 0; m < MC; m++) cfma2(acc[i][m], wv, cur[cl[m] * 64 + pr]);
+          for (int m = 0; m < MC; m++) cfma2(acc[i][m], wv, tile[cl[m] * 64 + pr]);
         }
       }
     }
@@ -322,17 +354,17 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         const bool neg = __popc(c[m] & T.smask) & 1;
         const unsigned pc = cl[m] ^ T.fl;
         if (REAL) {
-          const double wv = neg ? -T.coef.y : T.coef.y;
+          const S wv = (S)(neg ? -T.coef.y : T.coef.y);
 #pragma unroll
           for (int i = 0; i < 2; i++) {
-            const double2 p = cur[pc * 64 + rl[i]];
+            const V2 p = tile[pc * 64 + rl[i]];
             acc[i][m].x = fma(-wv, p.y, acc[i][m].x);
             acc[i][m].y = fma(wv, p.x, acc[i][m].y);
           }
         } else {
-          const double2 wv = neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef;
+          const V2 wv = to_v2<V2>(neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef);
 #pragma unroll
-          for (int i = 0; i < 2; i++) cfma2(acc[i][m], wv, cur[pc * 64 + rl[i]]);
+          for (int i = 0; i < 2; i++) cfma2(acc[i][m], wv, tile[pc * 64 + rl[i]]);
         }
       }
     }
@@ -347,13 +379,13 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         for (int m = 0; m < MC; m++) {
           if ((c[m] & T.cmask) != T.cval) continue;
           const bool neg = (sr + __popc(c[m] & T.smask)) & 1;
-          const double2 p = cur[(cl[m] ^ T.fl) * 64 + pr];
+          const V2 p = tile[(cl[m] ^ T.fl) * 64 + pr];
           if (REAL) {
-            const double wv = neg ? -T.coef.x : T.coef.x;
+            const S wv = (S)(neg ? -T.coef.x : T.coef.x);
             acc[i][m].x = fma(wv, p.x, acc[i][m].x);
             acc[i][m].y = fma(wv, p.y, acc[i][m].y);
           } else {
-            cfma2(acc[i][m], neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef, p);
+            cfma2(acc[i][m], to_v2<V2>(neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef), p);
           }
         }
       }
@@ -368,7 +400,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         for (int m = 0; m < MC; m++) {
           if ((c[m] & T.cmask) != T.cval) continue;
           const bool neg = (sr + __popc(c[m] & T.smask)) & 1;
-          cfma2(acc[i][m], neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef, cur[cl[m] * 64 + rl[i]]);
+          cfma2(acc[i][m], to_v2<V2>(neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef), tile[cl[m] * 64 + rl[i]]);
         }
       }
     }
@@ -399,7 +431,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
             pidx = (size_t)(c[m] ^ f) * D + (r[i] ^ f);
             sg = __popc(r[i] & T.smask) + __popc(c[m] & T.smask);
           }
-          cfma2(acc[i][m], (sg & 1) ? make_double2(-T.coef.x, -T.coef.y) : T.coef, __ldg(X + pidx));
+          cfma2(acc[i][m], to_v2<V2>((sg & 1) ? make_double2(-T.coef.x, -T.coef.y) : T.coef),
+                to_v2<V2>(__ldg(X + pidx)));
         }
       }
     }
@@ -409,11 +442,11 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
 #pragma unroll
       for (int m = 0; m < MC; m++) {
         const size_t idx = (size_t)c[m] * D + r[i];
-        const double2 Kv = acc[i][m];
         if (!P.last) {
-          P.accout[idx] = Kv;
+          reinterpret_cast<V2 *>(P.accout)[idx] = acc[i][m];
           continue;
         }
+        const double2 Kv = make_double2((double)acc[i][m].x, (double)acc[i][m].y);
         if (E.kout) E.kout[idx] = Kv;
         double2 u0 = make_double2(0.0, 0.0), u1 = u0, u2 = u0;
         if (E.nupd > 0) {
@@ -540,27 +573,32 @@ void encode_tma(const PassParams &pp, const double2 *x, CUtensorMap *map) {
   if (r != CUDA_SUCCESS) fail(9, "ERROR! cuTensorMapEncodeTiled failed (%d)\n", (int)r);
 }
 
-template <bool REAL, bool TMA, int NTHR, int CANON>
+template <bool REAL, bool TMA, int NTHR, int CANON, bool F32>
 void launch_pass(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e,
                  int grid, size_t smem, cudaStream_t s) {
   static bool done = false;
   if (!done) {
-    QCUDA(cudaFuncSetAttribute(k_qpass<REAL, TMA, NTHR, CANON>,
+    QCUDA(cudaFuncSetAttribute(k_qpass<REAL, TMA, NTHR, CANON, F32>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     done = true;
   }
-  k_qpass<REAL, TMA, NTHR, CANON><<<grid, NTHR, smem, s>>>(pp, map, x, e);
+  k_qpass<REAL, TMA, NTHR, CANON, F32><<<grid, NTHR, smem, s>>>(pp, map, x, e);
 }
 
-template <int CANON>
-void launch_canon(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e,
-                  int grid, size_t smem, cudaStream_t s) {
-  launch_pass<true, true, 1024, CANON>(pp, map, x, e, grid, smem, s);
-}
+template <bool F32>
+struct Canon {
+  template <int CANON>
+  static void launch(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e, int grid,
+                     size_t smem, cudaStream_t s) {
+    launch_pass<true, true, 1024, CANON, F32>(pp, map, x, e, grid, smem, s);
+  }
+};
 
 // canonical fast path: real mode, TMA, no general terms in this pass
+template <bool F32>
 void launch_canon_mask(int mask, const PassParams &pp, const CUtensorMap &map, const double2 *x,
                        const Epi &e, int grid, size_t smem, cudaStream_t s) {
+#define launch_canon Canon<F32>::template launch
   switch (mask) {
     case 0: launch_canon<0>(pp, map, x, e, grid, smem, s); break;
     case 1: launch_canon<1>(pp, map, x, e, grid, smem, s); break;
@@ -579,7 +617,9 @@ void launch_canon_mask(int mask, const PassParams &pp, const CUtensorMap &map, c
     case 14: launch_canon<14>(pp, map, x, e, grid, smem, s); break;
     default: launch_canon<15>(pp, map, x, e, grid, smem, s); break;
   }
+#undef launch_canon
 }
+
 
 int canon_mask(const PassParams &pp) {
   int m = 0;
@@ -590,6 +630,19 @@ int canon_mask(const PassParams &pp) {
     if (pp.gu[b] != 0) m |= 8;
   }
   return m;
+}
+
+template <bool F32>
+void launch_any_pass(PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e, int grid,
+                     size_t smem, cudaStream_t s) {
+  const bool tma = pp.tma != 0;
+  const bool only_canon = pp.real && tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 &&
+                          pp.nspill == 0;
+  if (only_canon) launch_canon_mask<F32>(canon_mask(pp), pp, map, x, e, grid, smem, s);
+  else if (pp.real && tma) launch_pass<true, true, 512, -1, F32>(pp, map, x, e, grid, smem, s);
+  else if (pp.real) launch_pass<true, false, 512, -1, F32>(pp, map, x, e, grid, smem, s);
+  else if (tma) launch_pass<false, true, 512, -1, F32>(pp, map, x, e, grid, smem, s);
+  else launch_pass<false, false, 512, -1, F32>(pp, map, x, e, grid, smem, s);
 }
 
 }  // namespace
@@ -715,7 +768,7 @@ bool check_program_error(DeviceProgram &P, cudaStream_t s) {
 // Runs the passes; `scratch` holds D^2 complex values when there are at
 // least two passes.
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
-                         const Epi &e, cudaStream_t s) {
+                         const Epi &e, cudaStream_t s, bool f32) {
   const int np = (int)passes.size();
   const long long nt = passes[0].ntiles;
   const int grid = (int)std::min<long long>(nt, num_sms());
@@ -728,13 +781,8 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
     const bool tma = pp.tma != 0;
     if (tma) encode_tma(pp, x, &map);
     const size_t smem = (size_t)((tma ? 3 : 2) * NEL + QMAX_GROUPS * 64) * sizeof(double2);
-    const bool only_canon = pp.real && tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 &&
-                            pp.nJx == 0 && pp.nspill == 0;
-    if (only_canon) launch_canon_mask(canon_mask(pp), pp, map, x, e, grid, smem, s);
-    else if (pp.real && tma) launch_pass<true, true, 512, -1>(pp, map, x, e, grid, smem, s);
-    else if (pp.real) launch_pass<true, false, 512, -1>(pp, map, x, e, grid, smem, s);
-    else if (tma) launch_pass<false, true, 512, -1>(pp, map, x, e, grid, smem, s);
-    else launch_pass<false, false, 512, -1>(pp, map, x, e, grid, smem, s);
+    if (f32) launch_any_pass<true>(pp, map, x, e, grid, smem, s);
+    else launch_any_pass<false>(pp, map, x, e, grid, smem, s);
     count_launch();
     QCUDA(cudaGetLastError());
   }

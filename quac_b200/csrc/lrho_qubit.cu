@@ -11,7 +11,7 @@
 // With all Hamiltonian coefficients purely imaginary and all jump rates
 // real (real couplings, Pauli X/Z and ladder operators) each partner costs
 // two FMAs instead of four.
-#include "common.h"
+#include "runtime.h"
 
 namespace quac {
 
@@ -269,7 +269,7 @@ void launch_lrho_any(const DeviceProgram &P, const double2 *x, const Epi &e, cud
       QCUDA(cudaMalloc(&M.scratch, n * sizeof(double2)));
       M.allocations.push_back(M.scratch);
     }
-    launch_qubit_passes(M.passes, x, M.scratch, e, s);
+    launch_qubit_passes(M.passes, x, M.scratch, e, s, options().lrho_f32 != 0);
   } else if (P.has_qubit) {
     launch_lrho_qubit(P, x, e, s);
   } else {

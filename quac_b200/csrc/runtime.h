@@ -36,6 +36,7 @@ struct Options {
   int64_t max_steps = -1;           // -1: use the caller's steps_max
   bool rtol_set = false, atol_set = false;
   int kernel_path = 0;              // see quac_set_kernel_path
+  int lrho_f32 = 0;                 // see quac_set_lrho_precision
   bool rk4_classic = false;         // rk_type "4classic": four-stage form instead of Horner
 };
 Options &options();

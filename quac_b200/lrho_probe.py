@@ -1,6 +1,6 @@
 """Applies L.rho a few times on the device (for profiling runs).
 
-    python -m quac_b200.lrho_probe --qubits 12 --reps 3 [--path 0|1|2]
+    python -m quac_b200.lrho_probe --qubits 12 --reps 3 [--path 0|1|2] [--fp32]
 
 Builds the open transverse-field Ising chain of the benchmark with the
 given number of qubits, allocates x and y with torch on cuda:0 and calls
@@ -19,10 +19,12 @@ def main():
     ap.add_argument("--qubits", type=int, default=12)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--path", type=int, default=0)
+    ap.add_argument("--fp32", action="store_true", help="complex64 contraction")
     a = ap.parse_args()
     q.lib()
     q.QuaC_initialize()
     q.set_kernel_path(a.path)
+    q.set_lrho_precision(1 if a.fp32 else 0)
     S = Builder(q)
     tfim(S, a.qubits)
     q.construct_matrix(S.qs)

@@ -462,3 +462,52 @@ def test_multipass_rk4_tfim9_matches_oracle(quac, oracle):
     assert _rel(rho.to_numpy(), yo) < 1e-12
     rho.destroy()
     S.qs.destroy()
+
+
+# complex64 contraction (multi-pass kernel): one L.x is held to 2e-6
+# relative (float rounding of tiles, coefficients and ~40 accumulated terms);
+# an integration keeps its FP64 state, so trace and populations stay within
+# 1e-6 of the complex128 run over a short horizon.
+def test_fp32_contraction_lx_matches_oracle(quac, oracle):
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.tfim(S, 9)
+    H.tfim(O, 9)
+    quac.construct_matrix(S.qs)
+    x = H.random_state(S.D, seed=4, hermitian=True)
+    quac.set_lrho_precision(1)
+    try:
+        y32 = quac.lrho_apply_host(S.qs, x)
+    finally:
+        quac.set_lrho_precision(0)
+    y64 = quac.lrho_apply_host(S.qs, x)
+    ref = O.liouvillian() @ x
+    assert _rel(y64, ref) < 1e-12
+    e = _rel(y32, ref)
+    assert 1e-10 < e < 2e-6
+    S.qs.destroy()
+
+
+def test_fp32_contraction_integration_error(quac):
+    outs = []
+    for prec in (0, 1):
+        S = H.ProductSystem(quac)
+        H.tfim(S, 9)
+        quac.construct_matrix(S.qs)
+        D = S.D
+        rho = quac.create_dm_sys(S.qs)
+        quac.add_to_qvec(rho, 1.0, 0, 0)
+        quac.assemble_qvec(rho)
+        quac.set_lrho_precision(prec)
+        quac.set_ts_options(rk_type="5dp", adapt_type="basic", rtol=1e-8, atol=1e-8)
+        try:
+            quac.time_step_sys(S.qs, rho, 0.0, 2.0, 0.01, 10 ** 6)
+        finally:
+            quac.set_lrho_precision(0)
+            quac.set_ts_options(rk_type="3bs", adapt_type="basic", rtol=5e-7, atol=5e-7)
+        outs.append(rho.to_numpy().reshape(D, D, order="F"))
+        rho.destroy()
+        S.qs.destroy()
+    a, b = outs
+    assert abs(np.trace(b) - 1.0) < 1e-6
+    assert np.abs(a.diagonal().real - b.diagonal().real).max() < 1e-6

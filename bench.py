@@ -246,6 +246,56 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=4):
     return out
 
 
+def precision_summary(q, qs, rho, x0, stream, steps, segment):
+    """12-qubit TFIM with complex64 contraction: the headline segment timed
+    again, and the full run of that workload (Dormand-Prince 5(4),
+    rtol = atol = 1e-8, t = 0..50 from |0...0><0...0|) in both precisions
+    with the errors of the complex64 run against the complex128 one."""
+    import torch
+    D = int(round(np.sqrt(x0.size)))
+    out = {}
+    q.set_lrho_precision(1)
+    rho.from_numpy(x0)
+    segment(0.0)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    t = 0.0
+    for _ in range(steps):
+        segment(t)
+        t += RK_STEPS * DT
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    out["lrho_gbs"] = steps * STAGES * 32.0 * D * D / (ms / 1e3) / 1e9
+    out["ms_per_step"] = ms / steps
+    q.set_lrho_precision(0)
+    states, secs = [], []
+    q.set_ts_options(rk_type="5dp", adapt_type="basic", rtol=1e-8, atol=1e-8)
+    for prec in (0, 1):
+        q.set_lrho_precision(prec)
+        z = np.zeros(D * D, dtype=np.complex128)
+        z[0] = 1.0
+        rho.from_numpy(z)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        q.time_step_sys(qs, rho, 0.0, 50.0, 0.01, 10 ** 7)
+        torch.cuda.synchronize()
+        secs.append(time.perf_counter() - t0)
+        states.append(rho.to_numpy().reshape(D, D, order="F"))
+    q.set_lrho_precision(0)
+    q.set_ts_options(rk_type="4", adapt_type="none", rtol=5e-7, atol=5e-7)
+    a, b = states
+    out["run_t50_seconds"] = {"fp64": secs[0], "fp32_contraction": secs[1]}
+    out["errors_vs_fp64"] = {
+        "trace": float(abs(np.trace(b) - np.trace(a))),
+        "population_max": float(np.abs(a.diagonal().real - b.diagonal().real).max()),
+        "state_rel_frobenius": float(np.linalg.norm(a - b) / np.linalg.norm(a)),
+        "purity": float(abs(np.vdot(b, b).real - np.vdot(a, a).real)),
+    }
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import quac_b200 as q
@@ -339,6 +389,9 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and world == 1 and not args.no_ensemble:
+        q.set_stream(qs, stream.cuda_stream)
+        out["fp32_contraction"] = precision_summary(q, qs, rho, x0, stream, args.steps, segment)
+        q.set_stream(qs, None)
         out["ensemble"] = ensemble_summary(q)
     q.set_ts_options(rk_type="3bs", adapt_type="basic")
     rho.destroy()

@@ -296,6 +296,76 @@ def precision_summary(q, qs, rho, x0, stream, steps, segment):
     return out
 
 
+def jc_summary(q, t_end=200.0, dt=0.01):
+    """Jaynes-Cummings (emitter 2 x cavity 10, QuaC's simple JC form): fixed
+    RK4 dt = 0.01 to t = 200 (20,000 steps) with the emitter and cavity
+    populations recorded by a monitor after every step."""
+    from quac_b200.systems import Builder, jc
+    S = Builder(q)
+    qb, cav = jc(S)
+    q.construct_matrix(S.qs)
+    rho = q.create_qvec_sys(S.qs)
+    q.add_to_qvec(rho, 1.0, 10, 10)
+    q.assemble_qvec(rho)
+    pops = []
+    q.set_ts_monitor_sys(S.qs, lambda step, t, v: pops.append(
+        (q.get_expectation_value_qvec(rho, qb.n).real, q.get_expectation_value_qvec(rho, cav.n).real)))
+    q.set_ts_options(rk_type="4", adapt_type="none")
+    t0 = time.perf_counter()
+    q.time_step_sys(S.qs, rho, 0.0, t_end, dt, 10 ** 7)
+    sec = time.perf_counter() - t0
+    q.set_ts_options(rk_type="3bs", adapt_type="basic")
+    q.set_ts_monitor_sys(S.qs, None)
+    out = {"workload": "jc_2x10_rk4_t200_monitored", "steps": len(pops) - 1, "seconds": sec,
+           "steps_per_s": (len(pops) - 1) / sec, "final_populations": {"emitter": pops[-1][0], "cavity": pops[-1][1]}}
+    rho.destroy()
+    S.qs.destroy()
+    return out
+
+
+def circuit_summary(q, nq=10, layers=40):
+    """Noisy 10-qubit random circuit on rho (D = 1024): per layer the gates
+    (superoperator convention, apply_circuit_to_qvec) and then 1.0 time unit
+    of Lindblad evolution (default adaptive BS3); fidelity against the ideal
+    state obtained by applying the same gates to a second, noiseless rho."""
+    from quac_b200.systems import Builder, noisy_circuit_layers, noisy_qubits
+    S = Builder(q)
+    noisy_qubits(S, nq)
+    q.construct_matrix(S.qs)
+    rho = q.create_dm_sys(S.qs)
+    ideal = q.create_dm_sys(S.qs)
+    for v in (rho, ideal):
+        q.add_to_qvec(v, 1.0, 0, 0)
+        q.assemble_qvec(v)
+    spec = noisy_circuit_layers(nq, layers)
+    circs = []
+    for layer in spec:
+        c = q.create_circuit(len(layer))
+        for g, qb, kw in layer:
+            c.add_gate(0.0, g, *qb, **kw)
+        circs.append(c)
+    t0 = time.perf_counter()
+    t = 0.0
+    for c in circs:
+        q.apply_circuit_to_qvec(S.qs, c, rho)
+        q.time_step_sys(S.qs, rho, t, t + 1.0, 0.1, 10 ** 6)
+        t += 1.0
+    sec = time.perf_counter() - t0
+    for c in circs:
+        q.apply_circuit_to_qvec(S.qs, c, ideal)
+    D = S.D
+    a = rho.to_numpy()
+    b = ideal.to_numpy()
+    fid = float(np.vdot(b, a).real)  # Tr(rho_ideal rho) for a pure rho_ideal
+    tr = complex(np.trace(a.reshape(D, D, order="F")))
+    out = {"workload": f"noisy_random_circuit_{nq}q_{layers}layers", "seconds": sec, "layers_per_s": layers / sec,
+           "fidelity_vs_ideal": fid, "trace_error": abs(tr - 1.0)}
+    rho.destroy()
+    ideal.destroy()
+    S.qs.destroy()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import quac_b200 as q
@@ -393,6 +463,8 @@ def run_ours(args, rank, world, local_rank):
         out["fp32_contraction"] = precision_summary(q, qs, rho, x0, stream, args.steps, segment)
         q.set_stream(qs, None)
         out["ensemble"] = ensemble_summary(q)
+        out["jc"] = jc_summary(q)
+        out["circuit"] = circuit_summary(q)
     q.set_ts_options(rk_type="3bs", adapt_type="basic")
     rho.destroy()
     qs.destroy()
@@ -406,7 +478,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the sections beside the headline (complex64, ensemble, JC, circuit)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -117,3 +117,48 @@ def excited_vacuum(nc):
     rho = np.zeros(D * D, dtype=np.complex128)
     rho[nc * D + nc] = 1.0
     return rho
+
+
+def noisy_circuit_layers(nq=10, layers=40):
+    """Gate lists of the noisy random-circuit workload: in layer l each qubit
+    q draws, from default_rng(1000 l + q), one of H, X, RZ(theta), U3(theta,
+    phi, lambda) with angles ~ U[0, 2 pi); then CNOTs on a random
+    nearest-neighbour matching from default_rng(l) (pairs (i, i+1) from a
+    random offset, each pair with probability 1/2, random orientation).
+    Returns a list of layers, each a list of (gate, qubits, kw)."""
+    out = []
+    for l in range(layers):
+        layer = []
+        for q in range(nq):
+            rng = np.random.default_rng(1000 * l + q)
+            k = int(rng.integers(4))
+            if k == 0:
+                layer.append(("HADAMARD", (q,), {}))
+            elif k == 1:
+                layer.append(("SIGMAX", (q,), {}))
+            elif k == 2:
+                layer.append(("RZ", (q,), dict(theta=float(rng.uniform(0, 2 * np.pi)))))
+            else:
+                th, ph, la = rng.uniform(0, 2 * np.pi, size=3)
+                layer.append(("U3", (q,), dict(theta=float(th), phi=float(ph), lam=float(la))))
+        rng = np.random.default_rng(l)
+        off = int(rng.integers(2))
+        for i in range(off, nq - 1, 2):
+            if rng.uniform() < 0.5:
+                c, t = (i, i + 1) if rng.uniform() < 0.5 else (i + 1, i)
+                layer.append(("CNOT", (c, t), {}))
+        out.append(layer)
+    return out
+
+
+def noisy_qubits(S, nq=10):
+    """nq qubits with amplitude damping gamma1 ~ U[5e-4, 2e-3] and dephasing
+    gamma_phi ~ U[2e-4, 1e-3] per qubit (default_rng(7))."""
+    rng = np.random.default_rng(7)
+    g1 = rng.uniform(5e-4, 2e-3, size=nq)
+    gp = rng.uniform(2e-4, 1e-3, size=nq)
+    qs = [S.op(2) for _ in range(nq)]
+    for i in range(nq):
+        S.lin(g1[i], qs[i].a)
+        S.lin(gp[i], qs[i].n)
+    return qs

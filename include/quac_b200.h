@@ -359,6 +359,16 @@ void quac_set_kernel_path(int path);
  * with the state, the RK stage combinations, the error norm and every
  * reduction kept in complex128.  Other kernels always run complex128. */
 int quac_set_lrho_precision(int precision);
+/* Hermitian mode of time_step_sys (no reference counterpart): 1 (default) =
+ * automatic: for a 12-qubit system on the multi-pass kernel whose terms
+ * preserve Hermiticity, integrated from a Hermitian state with no gate
+ * events inside the run, every L.x computes the blocks on and above the
+ * block diagonal only and writes the others as their conjugate transposes
+ * (half the outputs and most of the traffic); 0 = always compute every
+ * element. */
+int quac_set_hermitian_mode(int mode);
+/* Number of L.x applications that ran in Hermitian mode (diagnostics). */
+int64_t quac_hermitian_apply_count(void);
 /* Number of kernels this library has launched (diagnostics). */
 int64_t quac_kernel_launch_count(void);
 

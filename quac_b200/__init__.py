@@ -165,6 +165,8 @@ def lib():
         "quac_set_stream": (None, [P(_QsysStruct), vp]),
         "quac_set_kernel_path": (None, [ctypes.c_int]),
         "quac_set_lrho_precision": (ctypes.c_int, [ctypes.c_int]),
+        "quac_set_hermitian_mode": (ctypes.c_int, [ctypes.c_int]),
+        "quac_hermitian_apply_count": (i64, []),
         "VecGetSize": (ctypes.c_int, [vp, P(i64)]),
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
         "read_qvec_wf_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
@@ -671,6 +673,16 @@ def set_stream(qs, stream_ptr):
 def set_kernel_path(path):
     """0: default selection; 1: generic table kernel; 2: single-pass bit-mask kernel."""
     lib().quac_set_kernel_path(int(path))
+
+
+def set_hermitian_mode(mode):
+    """1 (default): Hermitian mode when it applies; 0: never."""
+    lib().quac_set_hermitian_mode(int(mode))
+    _check()
+
+
+def hermitian_apply_count():
+    return lib().quac_hermitian_apply_count()
 
 
 def set_lrho_precision(precision):

@@ -1181,6 +1181,12 @@ extern "C" void quac_set_kernel_path(int path) {
   options().kernel_path = path;
 }
 
+extern "C" int quac_set_hermitian_mode(int mode) {
+  if (mode != 0 && mode != 1) { fail(0, "ERROR! Hermitian mode must be 0 (off) or 1 (automatic)\n"); return 1; }
+  options().herm_mode = mode;
+  return 0;
+}
+
 extern "C" int quac_set_lrho_precision(int precision) {
   if (precision != 0 && precision != 1) { fail(0, "ERROR! L.rho precision must be 0 (FP64) or 1 (FP32 contraction)\n"); return 1; }
   options().lrho_f32 = precision;

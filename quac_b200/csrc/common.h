@@ -79,6 +79,10 @@ struct Epi {
   const double2 *ny;
   const double2 *nyn;
   double atol, rtol;
+  // nonzero: x (and therefore L x) is Hermitian and L preserves Hermiticity;
+  // the multi-pass kernel then computes the upper block triangle only and
+  // writes the rest as its conjugate transpose
+  int herm;
 };
 
 // Qubit fast path: every subsystem is two-level, so each operator product
@@ -119,6 +123,7 @@ struct PassParams {
   int ngroups;
   int nspill;            // cross-group terms handled with global loads (last pass)
   int ncanon;            // nonzero: canonical single-bit coefficients below are used
+  int herm_tiles;        // last pass only: work items are the blocks I <= J, mirrored
   long long ntiles;
   const double2 *dr, *dc, *gtab;
   const double2 *accin;  // running sum from earlier passes (nullptr: start from zero)
@@ -139,6 +144,7 @@ struct DeviceProgram {
   DevProg dev{};
   HostProg host;
   bool has_qubit = false;
+  bool herm_ok = false;            // L(X^H) = (L X)^H for every X (checked on the compiled tables)
   std::vector<PassParams> passes;  // non-empty: multi-pass qubit kernel
   double2 *scratch = nullptr;      // D^2 running sum for the passes
   int *errflag = nullptr;          // device word set by kernels whose waits time out
@@ -165,6 +171,10 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
 // Reads and clears the program's device error word; reports through fail().
 bool check_program_error(DeviceProgram &P, cudaStream_t s);
 void zero_epi(Epi &e);
+// L(X^H) = (L X)^H for all X, decided from the compiled tables (terms.cpp)
+bool hermiticity_preserving(const HostProg &hp);
+// relative Frobenius asymmetry ||X - X^H|| / ||X|| of a D x D matrix (lincomb.cu)
+double hermitian_asymmetry(const double2 *x, int64_t D, cudaStream_t s);
 // C[M x N] = act(A[M x K] B[N x K]^T + bias), TF32 tensor cores; K % 32 == 0 (mlp.cu)
 void launch_gemm_tf32(const float *A, const float *B, float *C, const float *bias, int M, int N, int K, int act,
                       int *err, cudaStream_t s);

@@ -66,6 +66,7 @@ struct Stepper {
   cudaStream_t s;
   int64_t n;
   double atol, rtol;
+  int herm;  // Hermitian mode of the multi-pass kernel (see Epi::herm)
 
   void stage(const double2 *X, std::initializer_list<std::tuple<double2 *, const double2 *, double>> upd,
              double *nsum = nullptr, int err_upd = 0, const double2 *ny = nullptr,
@@ -86,6 +87,7 @@ struct Stepper {
     e.nyn = nyn;
     e.atol = atol;
     e.rtol = rtol;
+    e.herm = herm;
     launch_lrho_any(*P, X, e, s);
   }
 };
@@ -116,8 +118,16 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
   vec_sync_to_device(v);
   QCUDA(cudaDeviceSynchronize());
 
-  Stepper st{qs, &PP, s, n, o.atol, o.rtol};
   std::vector<Event> events = x ? collect_events(qs, t0, tmax) : std::vector<Event>();
+  // Hermitian mode: L preserves Hermiticity (checked on the compiled
+  // tables), the multi-pass kernel runs, no gate lands inside this run, and
+  // the initial state is Hermitian to rounding; every stage then keeps the
+  // state exactly Hermitian (conjugate-transposed blocks are written, not
+  // computed)
+  int herm = 0;
+  if (o.herm_mode && PP.herm_ok && PP.has_qubit && !PP.passes.empty() && P.ncols == P.D && events.empty())
+    herm = hermitian_asymmetry(v->d, P.D, s) <= 1e-13 ? 1 : 0;
+  Stepper st{qs, &PP, s, n, o.atol, o.rtol, herm};
   size_t next_ev = 0;
   _p_TS ts;
   ts.t = t0;
@@ -159,6 +169,7 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
         Epi e;
         zero_epi(e);
         e.kout = K[st_i];
+        e.herm = herm;
         launch_lrho_any(PP, X, e, s);
       }
       // xs now holds the fifth-order solution (input of stage 7)

@@ -4,6 +4,8 @@
 //   sum_i (|out_i - base_i| / (atol + rtol * max(|base_i|, |ref_i|)))^2
 // (mode 1: out is not written, only the norm of sum_j coef_j in_j is taken
 // against base and ref).
+#include <cmath>
+
 #include "common.h"
 
 namespace quac {
@@ -63,6 +65,44 @@ int grid_of(int64_t n) {
   return (int)(b < 148 * 16 ? b : 148 * 16);
 }
 
+// sums[0] += ||A - B^H||^2 over the block, sums[1] += ||A||^2, where A is
+// the 32 x 32 block (bi, bj) of X and B the block (bj, bi)
+__global__ void k_herm_asym(const double2 *__restrict__ x, int64_t D, double *sums) {
+  __shared__ double2 tb[32][33];
+  __shared__ double red[2][8];
+  const int64_t r0 = (int64_t)blockIdx.x * 32, c0 = (int64_t)blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  // block (bj, bi) -> tb, element (c0 + i, r0 + j) stored at tb[j][i]
+  for (int i = ty; i < 32; i += 8) {
+    const int64_t row = c0 + tx, col = r0 + i;
+    tb[i][tx] = (row < D && col < D) ? x[col * D + row] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  double a2 = 0.0, d2 = 0.0;
+  for (int j = ty; j < 32; j += 8) {
+    const int64_t row = r0 + tx, col = c0 + j;
+    if (row < D && col < D) {
+      const double2 a = x[col * D + row];   // X[row, col]
+      const double2 b = tb[tx][j];          // X[col, row]
+      const double dx = a.x - b.x, dy = a.y + b.y;
+      d2 += dx * dx + dy * dy;
+      a2 += a.x * a.x + a.y * a.y;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d2 += __shfl_down_sync(0xffffffffu, d2, o);
+    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+  }
+  if (tx == 0) { red[0][ty] = d2; red[1][ty] = a2; }
+  __syncthreads();
+  if (tx == 0 && ty == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int k = 0; k < 8; k++) { s0 += red[0][k]; s1 += red[1][k]; }
+    atomicAdd(&sums[0], s0);
+    atomicAdd(&sums[1], s1);
+  }
+}
+
 }  // namespace
 
 void launch_lincomb(double2 *out, const double2 *base, int nin, const double2 *const *in,
@@ -93,6 +133,20 @@ void launch_lincomb_norm(const double2 *base, const double2 *ref, int nin, const
   k_lincomb<<<grid_of(n), NT, 0, s>>>(A, n);
   count_launch();
   QCUDA(cudaGetLastError());
+}
+
+double hermitian_asymmetry(const double2 *x, int64_t D, cudaStream_t s) {
+  double *d = nullptr;
+  double h[2] = {0.0, 0.0};
+  QCUDA(cudaMallocAsync(&d, 2 * sizeof(double), s));
+  QCUDA(cudaMemsetAsync(d, 0, 2 * sizeof(double), s));
+  const unsigned nb = (unsigned)((D + 31) / 32);
+  k_herm_asym<<<dim3(nb, nb), dim3(32, 8), 0, s>>>(x, D, d);
+  count_launch();
+  QCUDA(cudaMemcpyAsync(h, d, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  QCUDA(cudaFreeAsync(d, s));
+  QCUDA(cudaStreamSynchronize(s));
+  return h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0;
 }
 
 }  // namespace quac

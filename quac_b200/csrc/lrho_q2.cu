@@ -97,7 +97,18 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, u
 }
 
 // fixed (non-tile) bits of a work item: rows then columns
-__device__ __forceinline__ void tile_origin(long long t, int n, int lo, unsigned &rfix, unsigned &cfix) {
+__device__ __forceinline__ void tile_origin(long long t, int n, int lo, unsigned &rfix, unsigned &cfix,
+                                            int herm = 0) {
+  if (herm) {
+    // work item t = J (J + 1) / 2 + I over the blocks I <= J of the high bits (lo == 0)
+    long long J = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while ((J + 1) * (J + 2) / 2 <= t) J++;
+    while (J * (J + 1) / 2 > t) J--;
+    const long long I = t - J * (J + 1) / 2;
+    rfix = (unsigned)(I << 6);
+    cfix = (unsigned)(J << 6);
+    return;
+  }
   const int hi = lo + 6;
   const unsigned lowmask = (1u << lo) - 1u;
   const int nhigh = n - hi;
@@ -113,9 +124,9 @@ __device__ __forceinline__ void tile_origin(long long t, int n, int lo, unsigned
 }
 
 __device__ __forceinline__ void load_tile(double2 *buf, const double2 *__restrict__ X, long long t,
-                                          int n, int lo) {
+                                          int n, int lo, int herm = 0) {
   unsigned rfix, cfix;
-  tile_origin(t, n, lo, rfix, cfix);
+  tile_origin(t, n, lo, rfix, cfix, herm);
   const size_t D = (size_t)1 << n;
   for (int e = threadIdx.x; e < NEL; e += blockDim.x) {
     const unsigned cl = e >> 6, rl = e & 63;
@@ -128,7 +139,7 @@ __device__ __forceinline__ void load_tile(double2 *buf, const double2 *__restric
 __device__ __forceinline__ void tma_tile(const PassParams &P, const CUtensorMap *map, double2 *buf,
                                          uint64_t *bar, long long t) {
   unsigned rfix, cfix;
-  tile_origin(t, P.n, P.lo, rfix, cfix);
+  tile_origin(t, P.n, P.lo, rfix, cfix, P.herm_tiles);
   const unsigned long long F = (unsigned long long)rfix | ((unsigned long long)cfix << P.n);
   int c[5] = {0, 0, 0, 0, 0};
 #pragma unroll
@@ -181,7 +192,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
       }
     }
   } else {
-    if (blockIdx.x < P.ntiles) load_tile(sm, X, blockIdx.x, n, lo);
+    if (blockIdx.x < P.ntiles) load_tile(sm, X, blockIdx.x, n, lo, P.herm_tiles);
     cp_commit();
   }
   long long t = blockIdx.x;
@@ -203,7 +214,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
       }
     } else {
       const long long tn = t + gridDim.x;
-      if (tn < P.ntiles) load_tile(sm + ((it + 1) & 1) * NEL, X, tn, n, lo);
+      if (tn < P.ntiles) load_tile(sm + ((it + 1) & 1) * NEL, X, tn, n, lo, P.herm_tiles);
       cp_commit();
       cp_wait<1>();
       __syncthreads();
@@ -223,7 +234,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
       __syncthreads();
     }
     unsigned rfix, cfix;
-    tile_origin(t, n, lo, rfix, cfix);
+    tile_origin(t, n, lo, rfix, cfix, P.herm_tiles);
+    // an off-diagonal block also stands for its conjugate transpose
+    const bool mirror = P.herm_tiles && rfix != cfix;
     unsigned rl[2] = {(unsigned)lane, (unsigned)lane + 32u};
     unsigned cl[MC];
 #pragma unroll
@@ -469,7 +482,36 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
           const double2 y = E.ny[idx];
           const double2 yn = E.yn_upd == 0 ? u0 : (E.yn_upd == 1 ? u1 : (E.yn_upd == 2 ? u2 : E.nyn[idx]));
           const double q = cabs2d(ev) / (E.atol + E.rtol * fmax(cabs2d(y), cabs2d(yn)));
-          nloc += q * q;
+          nloc += mirror ? 2.0 * q * q : q * q;
+        }
+      }
+    }
+    if (P.last && P.herm_tiles) {
+      // off-diagonal block: write the conjugate-transposed block (J, I) of
+      // every output; diagonal block: rewrite its strictly lower triangle as
+      // the conjugate of the upper one and zero the imaginary part of its
+      // diagonal, so the state stays exactly Hermitian.  Through the tile
+      // buffer: element (r, c) staged at c*64 + (r ^ c), so that both the
+      // staging stores and the transposed reads are conflict-free
+      double2 *stg = cur;
+      double2 *dst[4];
+      int nd = 0;
+      if (E.kout) dst[nd++] = E.kout;
+      for (int u = 0; u < E.nupd; u++) dst[nd++] = E.out[u];
+      for (int o = 0; o < nd; o++) {
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+          for (int m = 0; m < MC; m++)
+            stg[cl[m] * 64 + (rl[i] ^ cl[m])] = dst[o][(size_t)c[m] * D + r[i]];
+        __syncthreads();
+        for (int e2 = threadIdx.x; e2 < NEL; e2 += PT) {
+          const unsigned a = e2 & 63u, b = e2 >> 6;
+          double2 v = stg[a * 64 + (b ^ a)];  // value at (row b, column a) of block (I, J)
+          v.y = -v.y;
+          if (mirror || a > b) dst[o][(size_t)(rfix | b) * D + (cfix | a)] = v;
+          else if (a == b) dst[o][(size_t)(rfix | b) * D + (cfix | a)] = make_double2(v.x, 0.0);
         }
       }
     }
@@ -485,6 +527,105 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
       for (int q = 0; q < PT / 32; q++) s += red[q];
       atomicAdd(E.nsum, s);
     }
+  }
+}
+
+// First pass (high six bits) when the last pass runs on the blocks I <= J
+// only: the running sum is needed just where the row's high bits do not
+// exceed the column's, i.e. on the upper triangle of every 64 x 64 tile of
+// this pass (2080 of 4096 outputs).  Canonical single-bit terms only.
+// Outputs are enumerated column by column over folded column pairs
+// (c, 63 - c): 65 per pair, consecutive threads on consecutive rows.
+template <int NTHR, int CANON, bool F32>
+__global__ void __launch_bounds__(NTHR, 1) k_qpass_hh(const __grid_constant__ PassParams P,
+                                                      const __grid_constant__ CUtensorMap tmap,
+                                                      const double2 *__restrict__ X) {
+  constexpr int PT = NTHR;
+  constexpr int NUP = 2080;
+  using V2 = typename std::conditional<F32, float2, double2>::type;
+  using S = typename std::conditional<F32, float, double>::type;
+  extern __shared__ __align__(128) double2 sm[];
+  __shared__ __align__(8) uint64_t bars[3];
+  const int n = P.n, lo = P.lo;
+  const size_t D = (size_t)1 << n;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 3; q++) mbar_init(&bars[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 2; q++) {
+      const long long tq = blockIdx.x + (long long)q * gridDim.x;
+      if (tq < P.ntiles) tma_tile(P, &tmap, sm + q * NEL, &bars[q], tq);
+    }
+  }
+  constexpr bool C_HL = CANON < 0 || (CANON & 1), C_HR = CANON < 0 || (CANON & 2);
+  constexpr bool C_GL = CANON < 0 || (CANON & 4), C_GU = CANON < 0 || (CANON & 8);
+  long long t = blockIdx.x;
+  for (int it = 0; t < P.ntiles; it++, t += gridDim.x) {
+    double2 *cur = sm + (it % 3) * NEL;
+    const long long t2 = t + 2ll * gridDim.x;
+    if (threadIdx.x == 0 && t2 < P.ntiles) tma_tile(P, &tmap, sm + ((it + 2) % 3) * NEL, &bars[(it + 2) % 3], t2);
+    const unsigned parity = (unsigned)((it / 3) & 1);
+    const unsigned long long t0 = global_ns();
+    bool timed_out = false;
+    while (!mbar_try_wait(&bars[it % 3], parity)) {
+      if (global_ns() - t0 > 2000000000ull) { timed_out = true; break; }
+    }
+    if (__syncthreads_or(timed_out)) {
+      if (threadIdx.x == 0 && P.errflag) atomicExch(P.errflag, 1);
+      return;
+    }
+    const V2 *tile = reinterpret_cast<const V2 *>(cur);
+    if (F32) {
+      double2 tmp[NEL / PT];
+#pragma unroll
+      for (int k2 = 0; k2 < NEL / PT; k2++) tmp[k2] = cur[threadIdx.x + k2 * PT];
+      __syncthreads();
+      float2 *c32 = reinterpret_cast<float2 *>(cur);
+#pragma unroll
+      for (int k2 = 0; k2 < NEL / PT; k2++)
+        c32[threadIdx.x + k2 * PT] = make_float2((float)tmp[k2].x, (float)tmp[k2].y);
+      __syncthreads();
+    }
+    unsigned rfix, cfix;
+    tile_origin(t, n, lo, rfix, cfix);
+    V2 *aout = reinterpret_cast<V2 *>(P.accout);
+    for (int e = threadIdx.x; e < NUP; e += PT) {  // NUP is a multiple of 32: whole warps
+      const int fc = e / 65, p = e - fc * 65;
+      unsigned rr, cc;
+      if (p < 64 - fc) { rr = (unsigned)p; cc = (unsigned)(63 - fc); }
+      else { rr = (unsigned)(p - (64 - fc)); cc = (unsigned)fc; }
+      S ax = 0, ay = 0;
+#pragma unroll
+      for (int b = 0; b < 6; b++) {
+        const unsigned f = 1u << b;
+        if (C_HL) {
+          const S hl = (S)P.hl[b];
+          const V2 q = tile[cc * 64 + (rr ^ f)];
+          ax = fma(-hl, q.y, ax);
+          ay = fma(hl, q.x, ay);
+        }
+        if (C_HR) {
+          const S hr = (S)P.hr[b];
+          const V2 q = tile[(cc ^ f) * 64 + rr];
+          ax = fma(-hr, q.y, ax);
+          ay = fma(hr, q.x, ay);
+        }
+        if (C_GL || C_GU) {
+          const bool rb = rr & f, cb = cc & f;
+          const S g = (rb != cb) ? (S)0 : (rb ? (C_GU ? (S)P.gu[b] : (S)0) : (C_GL ? (S)P.gl[b] : (S)0));
+          const V2 q = tile[(cc ^ f) * 64 + (rr ^ f)];
+          ax = fma(g, q.x, ax);
+          ay = fma(g, q.y, ay);
+        }
+      }
+      V2 v;
+      v.x = ax;
+      v.y = ay;
+      aout[(size_t)(cfix | (cc << lo)) * D + (rfix | (rr << lo))] = v;
+    }
+    __syncthreads();  // every thread is done with cur before it is refilled
   }
 }
 
@@ -645,7 +786,25 @@ void launch_any_pass(PassParams &pp, const CUtensorMap &map, const double2 *x, c
   else launch_pass<false, false, 512, -1, F32>(pp, map, x, e, grid, smem, s);
 }
 
+template <int CANON, bool F32>
+void launch_hh(const PassParams &pp, const CUtensorMap &map, const double2 *x, int grid, size_t smem,
+               cudaStream_t s) {
+  static bool done = false;
+  if (!done) {
+    QCUDA(cudaFuncSetAttribute(k_qpass_hh<1024, CANON, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
+    done = true;
+  }
+  k_qpass_hh<1024, CANON, F32><<<grid, 1024, smem, s>>>(pp, map, x);
+}
+
+bool canonical_only(const PassParams &pp) {
+  return pp.real && pp.tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 && pp.nspill == 0 &&
+         !pp.diag;
+}
+
 }  // namespace
+
 
 // Splits a compiled qubit program into passes.  Returns false if the
 // system does not suit the multi-pass kernel (n < 7 or too many terms).
@@ -767,25 +926,51 @@ bool check_program_error(DeviceProgram &P, cudaStream_t s) {
 
 // Runs the passes; `scratch` holds D^2 complex values when there are at
 // least two passes.
+static int64_t g_herm_applications = 0;
+
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
                          const Epi &e, cudaStream_t s, bool f32) {
   const int np = (int)passes.size();
   const long long nt = passes[0].ntiles;
   const int grid = (int)std::min<long long>(nt, num_sms());
+  // Hermitian mode: two passes whose first covers exactly bits 6..11 (12 qubits)
+  const bool herm = e.herm && np == 2 && passes[0].lo == 6 && passes[0].n == 12 && canonical_only(passes[0]) &&
+                    passes[1].lo == 0 && passes[1].last;
+  if (herm) g_herm_applications++;
   for (int p = 0; p < np; p++) {
     PassParams &pp = passes[p];
     pp.accin = p > 0 ? scratch : nullptr;
     pp.accout = (p < np - 1) ? scratch : nullptr;
+    const long long ntiles_full = pp.ntiles;
+    if (herm && p == 1) {
+      const long long T = 1ll << (pp.n - 6);
+      pp.herm_tiles = 1;
+      pp.ntiles = T * (T + 1) / 2;
+    }
     CUtensorMap map;
     memset(&map, 0, sizeof(map));
     const bool tma = pp.tma != 0;
     if (tma) encode_tma(pp, x, &map);
     const size_t smem = (size_t)((tma ? 3 : 2) * NEL + QMAX_GROUPS * 64) * sizeof(double2);
-    if (f32) launch_any_pass<true>(pp, map, x, e, grid, smem, s);
-    else launch_any_pass<false>(pp, map, x, e, grid, smem, s);
+    const int g = (int)std::min<long long>(pp.ntiles, num_sms());
+    if (herm && p == 0) {
+      const bool m7 = canon_mask(pp) == 7;
+      if (f32) { if (m7) launch_hh<7, true>(pp, map, x, g, smem, s); else launch_hh<-1, true>(pp, map, x, g, smem, s); }
+      else { if (m7) launch_hh<7, false>(pp, map, x, g, smem, s); else launch_hh<-1, false>(pp, map, x, g, smem, s); }
+    } else if (f32) {
+      launch_any_pass<true>(pp, map, x, e, g, smem, s);
+    } else {
+      launch_any_pass<false>(pp, map, x, e, g, smem, s);
+    }
+    pp.herm_tiles = 0;
+    pp.ntiles = ntiles_full;
     count_launch();
     QCUDA(cudaGetLastError());
   }
+  (void)grid;
 }
 
 }  // namespace quac
+
+// Number of L.x applications that ran in Hermitian mode (diagnostics).
+extern "C" int64_t quac_hermitian_apply_count(void) { return quac::g_herm_applications; }

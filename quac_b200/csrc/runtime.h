@@ -37,6 +37,7 @@ struct Options {
   bool rtol_set = false, atol_set = false;
   int kernel_path = 0;              // see quac_set_kernel_path
   int lrho_f32 = 0;                 // see quac_set_lrho_precision
+  int herm_mode = 1;                // see quac_set_hermitian_mode
   bool rk4_classic = false;         // rk_type "4classic": four-stage form instead of Horner
 };
 Options &options();

@@ -235,6 +235,67 @@ bool compile_host(qsystem qs, int mode, HostProg &hp) {
   return !has_error();
 }
 
+// L(X^H) = (L X)^H for every X.  With the compiled form
+//   (L X)[r,c] = d(r,c) X[r,c] + (M_L X)[r,c] + (X M_R)[r,c] + sum_t a_t[r] b_t[c] X[p_t(r), p_t(c)]
+// this holds when M_L = M_R^H, every jump pair has b_t = lambda conj(a_t)
+// with lambda real, the same for the diagonal products, and
+// dr[k] - conj(dc[k]) is one real constant (so d(c,r) = conj(d(r,c))).
+bool hermiticity_preserving(const HostProg &hp) {
+  const int D = hp.D;
+  double scale = 0.0;
+  auto upd = [&](cplx v) { scale = std::max(scale, std::abs(v)); };
+  std::unordered_map<uint64_t, cplx> ML, MR;  // key (row << 32) | col
+  for (size_t t = 0; t < hp.Lmap.size(); t++)
+    for (int r = 0; r < D; r++)
+      if (hp.Lmap[t][r] >= 0) {
+        ML[((uint64_t)r << 32) | (uint32_t)hp.Lmap[t][r]] += hp.Lval[t][r];
+        upd(hp.Lval[t][r]);
+      }
+  for (size_t t = 0; t < hp.Rmap.size(); t++)
+    for (int c = 0; c < D; c++)
+      if (hp.Rmap[t][c] >= 0) {
+        MR[((uint64_t)hp.Rmap[t][c] << 32) | (uint32_t)c] += hp.Rval[t][c];
+        upd(hp.Rval[t][c]);
+      }
+  for (auto &v : hp.dr) upd(v);
+  for (auto &v : hp.dc) upd(v);
+  const double tol = 1e-13 * std::max(scale, 1e-300);
+  auto transposed = [](uint64_t k) { return (k << 32) | (k >> 32); };
+  for (auto &kv : ML) {
+    auto it = MR.find(transposed(kv.first));
+    const cplx other = it == MR.end() ? cplx(0.0) : std::conj(it->second);
+    if (std::abs(kv.second - other) > tol) return false;
+  }
+  for (auto &kv : MR)
+    if (ML.find(transposed(kv.first)) == ML.end() && std::abs(kv.second) > tol) return false;
+  // products a[r] b[c]: b = lambda conj(a), lambda real
+  auto pair_ok = [&](const std::vector<cplx> &a, const std::vector<cplx> &b) {
+    cplx lam = 0.0;
+    bool have = false;
+    for (int k = 0; k < D; k++) {
+      if (std::abs(a[k]) > tol) {
+        const cplx l = b[k] / std::conj(a[k]);
+        if (!have) { lam = l; have = true; }
+        if (std::abs(l - lam) > 1e-12 * std::max(1.0, std::abs(lam))) return false;
+      } else if (std::abs(b[k]) > tol) {
+        return false;
+      }
+    }
+    return std::abs(lam.imag()) <= 1e-12 * std::max(1.0, std::abs(lam));
+  };
+  for (size_t t = 0; t < hp.Jmap.size(); t++)
+    if (!pair_ok(hp.Jrow[t], hp.Jcol[t])) return false;
+  for (size_t t = 0; t < hp.Jdrow.size(); t++)
+    if (!pair_ok(hp.Jdrow[t], hp.Jdcol[t])) return false;
+  if (!hp.dr.empty()) {
+    const cplx s0 = hp.dr[0] - std::conj(hp.dc[0]);
+    if (std::abs(s0.imag()) > tol) return false;
+    for (int k = 1; k < D; k++)
+      if (std::abs(hp.dr[k] - std::conj(hp.dc[k]) - s0) > tol) return false;
+  }
+  return true;
+}
+
 DeviceProgram *compile_terms(qsystem qs, int mode) {
   DeviceProgram *P = new DeviceProgram();
   HostProg &hp = P->host;
@@ -264,6 +325,7 @@ DeviceProgram *compile_terms(qsystem qs, int mode) {
     QCUDA(cudaMemset(P->errflag, 0, sizeof(int)));
     P->allocations.push_back(P->errflag);
     if (!plan_qubit_passes(*P, P->passes)) P->passes.clear();
+    if (P->passes.size() == 2) P->herm_ok = hermiticity_preserving(hp);
   }
   d.qubit_path = P->has_qubit ? 1 : 0;
   return P;

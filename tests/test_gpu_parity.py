@@ -511,3 +511,51 @@ def test_fp32_contraction_integration_error(quac):
     a, b = outs
     assert abs(np.trace(b) - 1.0) < 1e-6
     assert np.abs(a.diagonal().real - b.diagonal().real).max() < 1e-6
+
+
+# Hermitian mode (12-qubit TFIM, Hermitian start): the blocks below the block
+# diagonal are written as conjugate transposes instead of being computed; the
+# result must agree with the full computation to rounding for every scheme.
+@pytest.mark.parametrize("rk,adapt", [("4", "none"), ("3bs", "basic"), ("5dp", "basic")])
+def test_hermitian_mode_matches_full_computation(quac, rk, adapt):
+    outs, counts = [], []
+    for mode in (1, 0):
+        S = H.ProductSystem(quac)
+        H.tfim(S, 12)
+        quac.construct_matrix(S.qs)
+        D = S.D
+        rho = quac.create_dm_sys(S.qs)
+        rho.from_numpy(H.random_state(D, seed=21, hermitian=True))
+        quac.set_hermitian_mode(mode)
+        quac.set_ts_options(rk_type=rk, adapt_type=adapt)
+        c0 = quac.hermitian_apply_count()
+        try:
+            quac.time_step_sys(S.qs, rho, 0.0, 0.05, 0.01, 10 ** 6)
+        finally:
+            quac.set_hermitian_mode(1)
+            quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+        counts.append(quac.hermitian_apply_count() - c0)
+        outs.append(rho.to_numpy())
+        rho.destroy()
+        S.qs.destroy()
+    assert counts[0] > 0 and counts[1] == 0
+    assert _rel(outs[0], outs[1]) < 1e-12
+    y = outs[0].reshape(4096, 4096, order="F")
+    assert np.array_equal(y, y.conj().T) or np.abs(y - y.conj().T).max() < 1e-15 * np.abs(y).max()
+
+
+def test_hermitian_mode_not_used_for_non_hermitian_state(quac):
+    S = H.ProductSystem(quac)
+    H.tfim(S, 12)
+    quac.construct_matrix(S.qs)
+    rho = quac.create_dm_sys(S.qs)
+    rho.from_numpy(H.random_state(S.D, seed=22, hermitian=False))
+    quac.set_ts_options(rk_type="4", adapt_type="none")
+    c0 = quac.hermitian_apply_count()
+    try:
+        quac.time_step_sys(S.qs, rho, 0.0, 0.02, 0.01, 10 ** 6)
+    finally:
+        quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+    assert quac.hermitian_apply_count() == c0
+    rho.destroy()
+    S.qs.destroy()

@@ -182,7 +182,7 @@ def run_reference(args, rank, world):
                 "reference algorithm timed instead"}))
 
 
-def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=4):
+def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8):
     """Driven Jaynes-Cummings ensemble (4096 instances, n_c ~ U{5..40}, each
     evolved to t = 100 with its own Dormand-Prince 5(4) step): solves/s of
     the persistent batched kernel in FP64 and with complex64 right-hand-side
@@ -450,8 +450,9 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-                     "kernel": "k_qpass: one L.rho = 2 pass launches (high-qubit pass, then "
-                               "low-qubit pass with the fused RK stage epilogue)",
+                     "kernel": "Hermitian mode: k_qpass_hh (high-qubit pass, upper triangle of each "
+                               "tile) then k_qpass (low-qubit pass on the blocks I <= J with the fused RK "
+                               "stage epilogue and conjugate-transposed writes)",
                      "per": "one L.rho application (32*D^2 algorithmic bytes)"},
         "gpu_launches": int(launches),
         "clocks": clk,

@@ -427,11 +427,8 @@ def run_ours(args, rank, world, local_rank):
         q.time_step_host(qs, hp, 0.0, RK_STEPS * DT, DT, 10 ** 9)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3
-    ms_t = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(ms_t[0]), float(ms_t[1])
+    from quac_b200.replicas import max_over_ranks
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], device=dev)
     alg_bytes = 32.0 * n
     total_apps = args.steps * STAGES * world
     value = total_apps * alg_bytes / (ms / 1e3) / 1e9

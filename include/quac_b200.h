@@ -367,6 +367,11 @@ int quac_set_lrho_precision(int precision);
  * (half the outputs and most of the traffic); 0 = always compute every
  * element. */
 int quac_set_hermitian_mode(int mode);
+/* Restart length of the steady-state GMRES (default 100 as in solver.c;
+ * -ksp_gmres_restart on the QuaC_initialize command line does the same).
+ * Up to 1024: a long Krylov space resolves the slow Lindblad modes that
+ * stall GMRES(100), at (m+1) x D^2 x 16 bytes of device memory. */
+int quac_set_gmres_restart(int m);
 /* Number of L.x applications that ran in Hermitian mode (diagnostics). */
 int64_t quac_hermitian_apply_count(void);
 /* Number of kernels this library has launched (diagnostics). */

@@ -166,6 +166,7 @@ def lib():
         "quac_set_kernel_path": (None, [ctypes.c_int]),
         "quac_set_lrho_precision": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_hermitian_mode": (ctypes.c_int, [ctypes.c_int]),
+        "quac_set_gmres_restart": (ctypes.c_int, [ctypes.c_int]),
         "quac_hermitian_apply_count": (i64, []),
         "VecGetSize": (ctypes.c_int, [vp, P(i64)]),
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
@@ -673,6 +674,12 @@ def set_stream(qs, stream_ptr):
 def set_kernel_path(path):
     """0: default selection; 1: generic table kernel; 2: single-pass bit-mask kernel."""
     lib().quac_set_kernel_path(int(path))
+
+
+def set_gmres_restart(m):
+    """Restart length of the steady-state GMRES (default 100)."""
+    lib().quac_set_gmres_restart(int(m))
+    _check()
 
 
 def set_hermitian_mode(mode):

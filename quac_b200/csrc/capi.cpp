@@ -191,6 +191,7 @@ void QuaC_initialize(int argc, char **args) {
     else if (!strcmp(a, "-ts_rtol")) { o.rtol = atof(v); o.rtol_set = true; i++; }
     else if (!strcmp(a, "-ts_atol")) { o.atol = atof(v); o.atol_set = true; i++; }
     else if (!strcmp(a, "-ts_max_steps")) { o.max_steps = atoll(v); i++; }
+    else if (!strcmp(a, "-ksp_gmres_restart")) { o.gmres_restart = atoi(v); i++; }
   }
 }
 
@@ -1179,6 +1180,12 @@ extern "C" void quac_set_stream(qsystem qs, void *stream) {
 
 extern "C" void quac_set_kernel_path(int path) {
   options().kernel_path = path;
+}
+
+extern "C" int quac_set_gmres_restart(int m) {
+  if (m < 1 || m > 1024) { fail(0, "ERROR! GMRES restart must be in [1, 1024]\n"); return 1; }
+  options().gmres_restart = m;
+  return 0;
 }
 
 extern "C" int quac_set_hermitian_mode(int mode) {

@@ -19,6 +19,7 @@ namespace {
 
 constexpr int NT = 256;
 constexpr int CHUNK = 1024;  // elements of w staged per block
+constexpr int GMRES_MAXM = 1024;  // largest restart length
 
 __device__ __forceinline__ double2 cmuls(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -105,7 +106,7 @@ __global__ void k_reduce_rows(const double2 *__restrict__ partial, int nb, doubl
 // w[i] -= sum_k c[k] V_k[i]   (c = the projections just computed)
 __global__ void k_multiaxpy(const double2 *__restrict__ V, const double2 *__restrict__ c, int64_t n,
                             int nk, double2 *__restrict__ w, double sign) {
-  __shared__ double2 cs[128];
+  __shared__ double2 cs[GMRES_MAXM + 1];
   for (int k = threadIdx.x; k < nk; k += NT) cs[k] = c[k];
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
@@ -422,7 +423,7 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
   const DevProg &P = PP.dev;
   const int64_t n = (int64_t)P.D * P.ncols;
   cudaStream_t s = stream_of(qs);
-  if (m < 1 || m > 127) { fail(9, "ERROR! GMRES restart must be in [1, 127]\n"); return -1; }
+  if (m < 1 || m > GMRES_MAXM) { fail(9, "ERROR! GMRES restart must be in [1, %d]\n", GMRES_MAXM); return -1; }
   Gmres &G = gmres_for(qs);
   G.ensure(n, m);
   if (!x_is_guess) {
@@ -526,7 +527,7 @@ extern "C" PetscInt steady_state_sys(qsystem qs, qvec x) {
   if (has_error()) return -1;
   vec_sync_to_device(x->data);
   double res = 0;
-  const int64_t its = gmres_solve(qs, x->data->d, 1e-11, 100, 200000, false, &res);
+  const int64_t its = gmres_solve(qs, x->data->d, 1e-11, options().gmres_restart, 200000, false, &res);
   return has_error() ? -1 : its;
 }
 
@@ -555,7 +556,7 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
   {
     Gmres &G = gmres_for(qs);
     const int64_t n = (int64_t)PP.dev.D * PP.dev.D;
-    G.ensure(n, 100);
+    G.ensure(n, options().gmres_restart);
     apply_A(PP, x->data->d, G.w, s);
     k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.w, n);
     count_launch();
@@ -570,11 +571,12 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
     if (!(r_guess <= r_e0)) QCUDA(cudaMemcpyAsync(x->data->d, G.V, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
   }
   double res = 0;
-  int64_t its = gmres_solve(qs, x->data->d, 1e-11, 100, maxit_guided, true, &res, use ? &F : nullptr);
+  const int m = options().gmres_restart;
+  int64_t its = gmres_solve(qs, x->data->d, 1e-11, m, maxit_guided, true, &res, use ? &F : nullptr);
   F.release();
   if (its < 0) return -1;
   if (res > 1e-11) {
-    const int64_t more = gmres_solve(qs, x->data->d, 1e-11, 100, 200000, true, &res);
+    const int64_t more = gmres_solve(qs, x->data->d, 1e-11, m, 200000, true, &res);
     if (more < 0) return -1;
     its += more;
   }

@@ -171,6 +171,9 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
 // Reads and clears the program's device error word; reports through fail().
 bool check_program_error(DeviceProgram &P, cudaStream_t s);
 void zero_epi(Epi &e);
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` (once per kernel, device and size; thread safe).
+void ensure_smem(const void *func, size_t bytes);
 // L(X^H) = (L X)^H for all X, decided from the compiled tables (terms.cpp)
 bool hermiticity_preserving(const HostProg &hp);
 // relative Frobenius asymmetry ||X - X^H|| / ||X|| of a D x D matrix (lincomb.cu)

@@ -9,6 +9,8 @@
 // coefficient) are read once and reused for K elements, while the
 // per-column tables are warp-uniform broadcasts.  Partners that fall inside
 // the tile come from shared memory, the others from global memory (L2).
+#include <map>
+#include <mutex>
 #include "common.h"
 
 namespace quac {
@@ -164,6 +166,18 @@ __global__ void __launch_bounds__(NT) k_lrho(const DevProg P, const double2 *__r
 }
 
 }  // namespace
+
+void ensure_smem(const void *func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> done;
+  int dev = 0;
+  QCUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  size_t &have = done[std::make_pair(func, dev)];
+  if (have >= bytes) return;
+  QCUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  if (!has_error()) have = bytes;
+}
 
 void zero_epi(Epi &e) {
   memset(&e, 0, sizeof(Epi));

@@ -18,6 +18,7 @@
 #include <array>
 #include <cstring>
 #include <type_traits>
+#include <atomic>
 
 #include <cuda.h>
 
@@ -717,12 +718,7 @@ void encode_tma(const PassParams &pp, const double2 *x, CUtensorMap *map) {
 template <bool REAL, bool TMA, int NTHR, int CANON, bool F32>
 void launch_pass(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e,
                  int grid, size_t smem, cudaStream_t s) {
-  static bool done = false;
-  if (!done) {
-    QCUDA(cudaFuncSetAttribute(k_qpass<REAL, TMA, NTHR, CANON, F32>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    done = true;
-  }
+  ensure_smem((const void *)k_qpass<REAL, TMA, NTHR, CANON, F32>, smem);
   k_qpass<REAL, TMA, NTHR, CANON, F32><<<grid, NTHR, smem, s>>>(pp, map, x, e);
 }
 
@@ -789,12 +785,7 @@ void launch_any_pass(PassParams &pp, const CUtensorMap &map, const double2 *x, c
 template <int CANON, bool F32>
 void launch_hh(const PassParams &pp, const CUtensorMap &map, const double2 *x, int grid, size_t smem,
                cudaStream_t s) {
-  static bool done = false;
-  if (!done) {
-    QCUDA(cudaFuncSetAttribute(k_qpass_hh<1024, CANON, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
-    done = true;
-  }
+  ensure_smem((const void *)k_qpass_hh<1024, CANON, F32>, smem);
   k_qpass_hh<1024, CANON, F32><<<grid, 1024, smem, s>>>(pp, map, x);
 }
 
@@ -926,7 +917,7 @@ bool check_program_error(DeviceProgram &P, cudaStream_t s) {
 
 // Runs the passes; `scratch` holds D^2 complex values when there are at
 // least two passes.
-static int64_t g_herm_applications = 0;
+static std::atomic<int64_t> g_herm_applications{0};
 
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
                          const Epi &e, cudaStream_t s, bool f32) {
@@ -973,4 +964,4 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
 }  // namespace quac
 
 // Number of L.x applications that ran in Hermitian mode (diagnostics).
-extern "C" int64_t quac_hermitian_apply_count(void) { return quac::g_herm_applications; }
+extern "C" int64_t quac_hermitian_apply_count(void) { return quac::g_herm_applications.load(); }

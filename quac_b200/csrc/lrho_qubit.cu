@@ -231,12 +231,7 @@ void launch_q(const QParams &qp, const double2 *x, const Epi &e, cudaStream_t s)
   constexpr int TC = 8 * M;
   const int D = 1 << qp.prog.n;
   const size_t smem = (size_t)(TC * 64 + 64 + TC + qp.prog.ngroups * 64) * sizeof(double2);
-  static bool attr_set = false;
-  if (!attr_set) {
-    QCUDA(cudaFuncSetAttribute(k_lrho_qubit<M, REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem + 4096));
-    attr_set = true;
-  }
+  ensure_smem((const void *)k_lrho_qubit<M, REAL>, smem + 4096);
   dim3 grid(D / 64, D / TC);
   k_lrho_qubit<M, REAL><<<grid, QNT, smem, s>>>(qp, x, e);
 }

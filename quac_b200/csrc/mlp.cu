@@ -201,12 +201,8 @@ __global__ void __launch_bounds__(128) k_gemm_tf32(const float *__restrict__ A, 
 // C = act(A B^T + bias) on device buffers; K must be a multiple of 32.
 void launch_gemm_tf32(const float *A, const float *B, float *C, const float *bias, int M, int N, int K, int act,
                       int *err, cudaStream_t s) {
-  static bool attr = false;
   const int smem = 4 * TILE_BYTES;
-  if (!attr) {
-    QCUDA(cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
-  }
+  ensure_smem((const void *)k_gemm_tf32, smem);
   dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
   k_gemm_tf32<<<grid, 128, smem, s>>>(A, B, C, bias, M, N, K, act, err);
   count_launch();

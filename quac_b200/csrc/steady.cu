@@ -8,6 +8,9 @@
 // kernels per pass (multi-dot, multi-axpy), repeated once (CGS2).  Only the
 // (m+1) x m Hessenberg matrix lives on the host.
 #include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <cstring>
 #include <vector>
 
@@ -295,10 +298,25 @@ struct Gmres {
   }
 };
 
-static Gmres &gmres_for(qsystem) {
-  static Gmres g;  // one solver workspace per process
-  return g;
+// One solver workspace per device; the steady-state entry points hold its
+// lock for the whole solve, so solves on one device run one at a time.
+struct GmresSlot {
+  Gmres g;
+  std::mutex mu;
+};
+
+static GmresSlot &gmres_slot() {
+  static std::mutex mu;
+  static std::map<int, std::unique_ptr<GmresSlot>> slots;
+  int dev = 0;
+  QCUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  std::unique_ptr<GmresSlot> &p = slots[dev];
+  if (!p) p.reset(new GmresSlot());
+  return *p;
 }
+
+static Gmres &gmres_for(qsystem) { return gmres_slot().g; }
 
 // A x with A = L + e0 vec(I)^T
 static void apply_A(const DeviceProgram &PP, const double2 *x, double2 *y, cudaStream_t s) {
@@ -526,6 +544,7 @@ extern "C" PetscInt steady_state_sys(qsystem qs, qvec x) {
   if (!qs->mat_allocated) construct_matrix(qs);
   if (has_error()) return -1;
   vec_sync_to_device(x->data);
+  std::lock_guard<std::mutex> lk(gmres_slot().mu);
   double res = 0;
   const int64_t its = gmres_solve(qs, x->data->d, 1e-11, options().gmres_restart, 200000, false, &res);
   return has_error() ? -1 : its;
@@ -546,6 +565,7 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
   ensure_program(qs);
   const DeviceProgram &PP = *qs->impl->prog;
   cudaStream_t s = stream_of(qs);
+  std::lock_guard<std::mutex> lk(gmres_slot().mu);
   Deflation F;
   const bool use = kd > 0;
   if (use && !build_deflation(PP, reinterpret_cast<const std::complex<double> *>(U_host), (int)kd, F, s)) {

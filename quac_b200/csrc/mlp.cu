@@ -4,11 +4,13 @@
 //   C[M x N] = act(A[M x K] . B[N x K]^T + bias[N])     (both operands K-major)
 //
 // One CTA of 128 threads computes a 128 x 128 output tile.  A and B tiles of
-// 32 K-columns are staged in shared memory in the canonical no-swizzle
-// K-major layout (8-row x 16-byte core matrices: the two 16-byte K chunks of
-// one MMA are LBO apart, consecutive 8-row groups SBO apart); one elected
-// thread issues four tcgen05.mma (K = 8 each) per stage and commits them to
-// that stage's mbarrier, so the loads of the next stage overlap the MMAs.
+// 32 K-columns are copied by cp.async (16 bytes per request, zero-filled past
+// the matrix edge) straight into the canonical no-swizzle K-major layout
+// (8-row x 16-byte core matrices: the two 16-byte K chunks of one MMA are
+// LBO apart, consecutive 8-row groups SBO apart), NST stages deep; one
+// elected thread issues four tcgen05.mma (K = 8 each) per stage and commits
+// them to that stage's mbarrier, which frees the stage for the copy NST - 1
+// steps ahead.
 // The accumulator (128 lanes x 128 columns of FP32) is read back with
 // tcgen05.ld; bias and activation are fused into that epilogue.
 //
@@ -23,6 +25,7 @@ namespace {
 
 constexpr int BM = 128, BN = 128, BK = 32;
 constexpr int TILE_BYTES = BM * BK * 4;  // 16 KB per operand per stage
+constexpr int NST = 3;                   // pipeline stages (96 KB: two CTAs per SM)
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -84,7 +87,8 @@ __device__ __forceinline__ uint32_t tile_off(int row, int k) {
   return (uint32_t)((k >> 2) * (BM * 16) + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
 }
 
-// rows [r0, r0 + 128) x k [k0, k0 + 32) of a row-major R x K matrix -> tile (zero past R)
+// rows [r0, r0 + 128) x k [k0, k0 + 32) of a row-major R x K matrix -> tile,
+// asynchronously (zero past R)
 __device__ __forceinline__ void load_tile(unsigned char *tile, const float *__restrict__ src, int R, int K, int r0,
                                           int k0) {
   // 128 rows x 8 chunks of 4 floats = 1024 chunks, 8 per thread
@@ -92,9 +96,11 @@ __device__ __forceinline__ void load_tile(unsigned char *tile, const float *__re
   for (int i = 0; i < 8; i++) {
     const int q = threadIdx.x + i * 128;
     const int row = q >> 3, chunk = q & 7;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (r0 + row < R) v = *reinterpret_cast<const float4 *>(src + (size_t)(r0 + row) * K + k0 + chunk * 4);
-    *reinterpret_cast<float4 *>(tile + tile_off(row, chunk * 4)) = v;
+    const bool in = r0 + row < R;
+    const float *g = in ? src + (size_t)(r0 + row) * K + k0 + chunk * 4 : src;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(tile + tile_off(row, chunk * 4))),
+                 "l"(g), "r"(in ? 16 : 0)
+                 : "memory");
   }
 }
 
@@ -102,12 +108,12 @@ __global__ void __launch_bounds__(128) k_gemm_tf32(const float *__restrict__ A, 
                                                    float *__restrict__ C, const float *__restrict__ bias, int M,
                                                    int N, int K, int act, int *err) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ __align__(8) uint64_t bars[NST];
   __shared__ uint32_t tmem_slot;
-  unsigned char *As[2] = {sm, sm + 2 * TILE_BYTES};
-  unsigned char *Bs[2] = {sm + TILE_BYTES, sm + 3 * TILE_BYTES};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  auto As = [&](int st) { return sm + st * 2 * TILE_BYTES; };
+  auto Bs = [&](int st) { return sm + st * 2 * TILE_BYTES + TILE_BYTES; };
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -115,8 +121,8 @@ __global__ void __launch_bounds__(128) k_gemm_tf32(const float *__restrict__ A, 
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < 2; s++)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[s])));
+    for (int st = 0; st < NST; st++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[st])));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -127,13 +133,18 @@ __global__ void __launch_bounds__(128) k_gemm_tf32(const float *__restrict__ A, 
   const int nk = K / BK;
   bool ok = true;
 
-  for (int kb = 0; kb < nk && ok; kb++) {
-    const int s = kb & 1;
-    if (kb >= 2) ok = mbar_wait(smem_u32(&bars[s]), ((kb - 2) >> 1) & 1, err);  // MMAs of kb-2 done
-    ok = __syncthreads_and(ok);
-    if (!ok) break;
-    load_tile(As[s], A, M, K, m0, kb * BK);
-    load_tile(Bs[s], B, N, K, n0, kb * BK);
+  // prologue: stages 0 .. NST-2 in flight (one commit group each, empty past nk)
+  for (int st = 0; st < NST - 1; st++) {
+    if (st < nk) {
+      load_tile(As(st), A, M, K, m0, st * BK);
+      load_tile(Bs(st), B, N, K, n0, st * BK);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (int kb = 0; kb < nk; kb++) {
+    const int st = kb % NST;
+    // stage kb has landed (at most NST-2 younger groups pending)
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(NST - 2) : "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -141,8 +152,8 @@ __global__ void __launch_bounds__(128) k_gemm_tf32(const float *__restrict__ A, 
       asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
       for (int k8 = 0; k8 < BK / 8; k8++) {
-        const uint64_t ad = smem_desc(smem_u32(As[s]) + k8 * 2 * (BM * 16), BM * 16, 128);
-        const uint64_t bd = smem_desc(smem_u32(Bs[s]) + k8 * 2 * (BN * 16), BN * 16, 128);
+        const uint64_t ad = smem_desc(smem_u32(As(st)) + k8 * 2 * (BM * 16), BM * 16, 128);
+        const uint64_t bd = smem_desc(smem_u32(Bs(st)) + k8 * 2 * (BN * 16), BN * 16, 128);
         const uint32_t acc = (kb > 0 || k8 > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -151,15 +162,22 @@ __global__ void __launch_bounds__(128) k_gemm_tf32(const float *__restrict__ A, 
             "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(&bars[s])));
+          smem_u32(&bars[st])));
     }
+    // refill the stage used by step kb-1 with step kb+NST-1, once its MMAs are done
+    const int kn = kb + NST - 1;
+    if (kn < nk) {
+      if (kb >= 1) ok = mbar_wait(smem_u32(&bars[(kb - 1) % NST]), ((kb - 1) / NST) & 1, err);
+      ok = __syncthreads_and(ok);
+      if (!ok) break;
+      load_tile(As(kn % NST), A, M, K, m0, kn * BK);
+      load_tile(Bs(kn % NST), B, N, K, n0, kn * BK);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
-  // wait for the last one or two stages still in flight
-  if (ok && nk >= 1) {
-    const int kb = nk - 1;
-    ok = mbar_wait(smem_u32(&bars[kb & 1]), (kb >> 1) & 1, err);
-    if (ok && nk >= 2) ok = mbar_wait(smem_u32(&bars[(kb - 1) & 1]), ((kb - 1) >> 1) & 1, err);
-  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  // the last commit covers every MMA issued before it
+  if (ok && nk >= 1) ok = mbar_wait(smem_u32(&bars[(nk - 1) % NST]), ((nk - 1) / NST) & 1, err);
   ok = __syncthreads_and(ok);
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (ok) {
@@ -201,7 +219,7 @@ __global__ void __launch_bounds__(128) k_gemm_tf32(const float *__restrict__ A, 
 // C = act(A B^T + bias) on device buffers; K must be a multiple of 32.
 void launch_gemm_tf32(const float *A, const float *B, float *C, const float *bias, int M, int N, int K, int act,
                       int *err, cudaStream_t s) {
-  const int smem = 4 * TILE_BYTES;
+  const int smem = NST * 2 * TILE_BYTES;
   ensure_smem((const void *)k_gemm_tf32, smem);
   dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
   k_gemm_tf32<<<grid, 128, smem, s>>>(A, B, C, bias, M, N, K, act, err);

@@ -28,7 +28,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libquac_b200.so")
+# QUAC_B200_LIB selects another build of the library (e.g. to compare two builds)
+LIB_PATH = os.environ.get("QUAC_B200_LIB") or os.path.join(_HERE, "libquac_b200.so")
 
 # op_type, qvec_type, gate_type (include/quac_b200.h)
 RAISE, NUMBER, LOWER, VEC, SIGMA_X, SIGMA_Y, SIGMA_Z, IDENTITY, OTHER = -1, 0, 1, 2, 3, 4, 5, 6, 7

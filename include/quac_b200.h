@@ -372,6 +372,14 @@ int quac_set_hermitian_mode(int mode);
  * Up to 1024: a long Krylov space resolves the slow Lindblad modes that
  * stall GMRES(100), at (m+1) x D^2 x 16 bytes of device memory. */
 int quac_set_gmres_restart(int m);
+/* Precision of the steady-state GMRES basis (no reference counterpart;
+ * solver.c runs KSPGMRES in PETSc's complex128).  0 (default): complex128.
+ * 1: FP32 inner / FP64 refined: the Krylov vectors are stored in complex64
+ * (half the Gram-Schmidt traffic), while L.x, the projections, the
+ * iterate and the residual b - A x formed at every restart stay
+ * complex128, so each restart refines the solution to the same
+ * complex128 tolerance. */
+int quac_set_gmres_precision(int precision);
 /* Number of L.x applications that ran in Hermitian mode (diagnostics). */
 int64_t quac_hermitian_apply_count(void);
 /* Number of kernels this library has launched (diagnostics). */

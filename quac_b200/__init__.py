@@ -168,6 +168,7 @@ def lib():
         "quac_set_lrho_precision": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_hermitian_mode": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_restart": (ctypes.c_int, [ctypes.c_int]),
+        "quac_set_gmres_precision": (ctypes.c_int, [ctypes.c_int]),
         "quac_hermitian_apply_count": (i64, []),
         "VecGetSize": (ctypes.c_int, [vp, P(i64)]),
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
@@ -680,6 +681,13 @@ def set_kernel_path(path):
 def set_gmres_restart(m):
     """Restart length of the steady-state GMRES (default 100)."""
     lib().quac_set_gmres_restart(int(m))
+    _check()
+
+
+def set_gmres_precision(precision):
+    """0 (default): complex128 GMRES basis; 1: complex64 basis (FP32 inner),
+    complex128 residual and iterate at every restart (FP64 refined)."""
+    lib().quac_set_gmres_precision(int(precision))
     _check()
 
 

@@ -1188,6 +1188,12 @@ extern "C" int quac_set_gmres_restart(int m) {
   return 0;
 }
 
+extern "C" int quac_set_gmres_precision(int precision) {
+  if (precision != 0 && precision != 1) { fail(0, "ERROR! GMRES precision must be 0 (FP64) or 1 (FP32 inner)\n"); return 1; }
+  options().gmres_f32 = precision;
+  return 0;
+}
+
 extern "C" int quac_set_hermitian_mode(int mode) {
   if (mode != 0 && mode != 1) { fail(0, "ERROR! Hermitian mode must be 0 (off) or 1 (automatic)\n"); return 1; }
   options().herm_mode = mode;

@@ -38,6 +38,7 @@ struct Options {
   int kernel_path = 0;              // see quac_set_kernel_path
   int lrho_f32 = 0;                 // see quac_set_lrho_precision
   int herm_mode = 1;                // see quac_set_hermitian_mode
+  int gmres_f32 = 0;                // see quac_set_gmres_precision
   int gmres_restart = 100;          // -ksp_gmres_restart (solver.c uses PETSc's default 100 via KSPGMRESSetRestart)
   bool rk4_classic = false;         // rk_type "4classic": four-stage form instead of Horner
 };

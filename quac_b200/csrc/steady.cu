@@ -12,6 +12,7 @@
 #include <memory>
 #include <mutex>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "runtime.h"
@@ -27,6 +28,16 @@ constexpr int GMRES_MAXM = 1024;  // largest restart length
 __device__ __forceinline__ double2 cmuls(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
+
+// Krylov basis elements: complex128, or complex64 in the FP32-inner solver
+// (every product and sum is still formed in double precision).
+__device__ __forceinline__ double2 ldv(const double2 *p) { return *p; }
+__device__ __forceinline__ double2 ldv(const float2 *p) {
+  const float2 v = *p;
+  return make_double2((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ void stv(double2 *p, double2 v) { *p = v; }
+__device__ __forceinline__ void stv(float2 *p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
 
 // y[0] += sum_i x[i*(D+1)]  (the stabilising trace row)
 __global__ void k_trace_add(const double2 *__restrict__ x, double2 *__restrict__ y, int64_t D) {
@@ -50,36 +61,35 @@ __global__ void k_trace_add(const double2 *__restrict__ x, double2 *__restrict__
   }
 }
 
-// partial[k*nb + blk] = sum over this block's chunk of conj(V_k[i]) w[i]
-__global__ void k_multidot(const double2 *__restrict__ V, const double2 *__restrict__ w, int64_t n,
+// partial[k*nb + blk] = sum over this block's chunk of conj(V_k[i]) w[i].
+// The chunk of w is staged in shared memory; each warp then takes one basis
+// vector k = blockIdx.y * 8 + warp, so all projections run side by side
+// (grid nb x ceil(nk / 8)) instead of one after another.
+template <typename VT>
+__global__ void k_multidot(const VT *__restrict__ V, const double2 *__restrict__ w, int64_t n,
                            int nk, double2 *__restrict__ partial) {
   __shared__ double2 ws[CHUNK];
-  __shared__ double2 red[2][NT / 32];
   const int64_t i0 = (int64_t)blockIdx.x * CHUNK;
   const int len = (int)min((int64_t)CHUNK, n - i0);
   for (int i = threadIdx.x; i < len; i += NT) ws[i] = w[i0 + i];
   __syncthreads();
-  for (int k = 0; k < nk; k++) {
-    const double2 *vk = V + (size_t)k * n + i0;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int i = threadIdx.x; i < len; i += NT) {
-      double2 a = vk[i];
-      a.y = -a.y;
-      const double2 p = cmuls(a, ws[i]);
-      acc.x += p.x; acc.y += p.y;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-      acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-    }
-    if ((threadIdx.x & 31) == 0) red[k & 1][threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double2 s = make_double2(0.0, 0.0);
-      for (int q = 0; q < NT / 32; q++) { s.x += red[k & 1][q].x; s.y += red[k & 1][q].y; }
-      partial[(size_t)k * gridDim.x + blockIdx.x] = s;
-    }
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.y * (NT / 32) + (threadIdx.x >> 5);
+  if (k >= nk) return;
+  const VT *vk = V + (size_t)k * n + i0;
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 4
+  for (int i = lane; i < len; i += 32) {
+    double2 a = ldv(vk + i);
+    a.y = -a.y;
+    const double2 p = cmuls(a, ws[i]);
+    acc.x += p.x; acc.y += p.y;
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+  }
+  if (lane == 0) partial[(size_t)k * gridDim.x + blockIdx.x] = acc;
 }
 
 // h[k] (+)= sum_b partial[k*nb + b]; one block per k.  accumulate != 0 adds.
@@ -107,7 +117,8 @@ __global__ void k_reduce_rows(const double2 *__restrict__ partial, int nb, doubl
 }
 
 // w[i] -= sum_k c[k] V_k[i]   (c = the projections just computed)
-__global__ void k_multiaxpy(const double2 *__restrict__ V, const double2 *__restrict__ c, int64_t n,
+template <typename VT>
+__global__ void k_multiaxpy(const VT *__restrict__ V, const double2 *__restrict__ c, int64_t n,
                             int nk, double2 *__restrict__ w, double sign) {
   __shared__ double2 cs[GMRES_MAXM + 1];
   for (int k = threadIdx.x; k < nk; k += NT) cs[k] = c[k];
@@ -115,7 +126,7 @@ __global__ void k_multiaxpy(const double2 *__restrict__ V, const double2 *__rest
   for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
     double2 acc = w[i];
     for (int k = 0; k < nk; k++) {
-      const double2 p = cmuls(cs[k], V[(size_t)k * n + i]);
+      const double2 p = cmuls(cs[k], ldv(V + (size_t)k * n + i));
       acc.x = fma(sign, p.x, acc.x);
       acc.y = fma(sign, p.y, acc.y);
     }
@@ -123,11 +134,62 @@ __global__ void k_multiaxpy(const double2 *__restrict__ V, const double2 *__rest
   }
 }
 
-// out = in * s (s real), returns nothing; also used to copy (s = 1)
-__global__ void k_scale(const double2 *__restrict__ in, double2 *__restrict__ out, int64_t n, double s) {
+// w[i] -= sum_k c[k] V_k[i], and npart[block] = sum over the block's i of |w[i]|^2
+// (the second Gram-Schmidt pass fused with the norm of the result).
+template <typename VT>
+__global__ void k_multiaxpy_norm(const VT *__restrict__ V, const double2 *__restrict__ c, int64_t n,
+                                 int nk, double2 *__restrict__ w, double *__restrict__ npart) {
+  __shared__ double2 cs[GMRES_MAXM + 1];
+  __shared__ double red[NT / 32];
+  for (int k = threadIdx.x; k < nk; k += NT) cs[k] = c[k];
+  __syncthreads();
+  double ss = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
-    const double2 v = in[i];
-    out[i] = make_double2(v.x * s, v.y * s);
+    double2 acc = w[i];
+    for (int k = 0; k < nk; k++) {
+      const double2 p = cmuls(cs[k], ldv(V + (size_t)k * n + i));
+      acc.x -= p.x;
+      acc.y -= p.y;
+    }
+    w[i] = acc;
+    ss = fma(acc.x, acc.x, fma(acc.y, acc.y, ss));
+  }
+  for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ss;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < NT / 32; q++) t += red[q];
+    npart[blockIdx.x] = t;
+  }
+}
+
+// h[k] += h2[k] for k < nk; h[nk] = (sqrt(sum npart), 0).  One block.
+__global__ void k_arnoldi_finish(double2 *__restrict__ h, const double2 *__restrict__ h2, int nk,
+                                 const double *__restrict__ npart, int nparts) {
+  __shared__ double red[NT / 32];
+  for (int k = threadIdx.x; k < nk; k += NT) {
+    h[k].x += h2[k].x;
+    h[k].y += h2[k].y;
+  }
+  double ss = 0.0;
+  for (int b = threadIdx.x; b < nparts; b += NT) ss += npart[b];
+  for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ss;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < NT / 32; q++) t += red[q];
+    h[nk] = make_double2(sqrt(t), 0.0);
+  }
+}
+
+// out = in * s (s real); also used to copy and convert (s = 1)
+template <typename TI, typename TO>
+__global__ void k_scale(const TI *__restrict__ in, TO *__restrict__ out, int64_t n, double s) {
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    const double2 v = ldv(in + i);
+    stv(out + i, make_double2(v.x * s, v.y * s));
   }
 }
 
@@ -192,8 +254,8 @@ __global__ void k_defl_proj(const double2 *__restrict__ X, const double2 *__rest
   }
 }
 
-// z = sum_b partial[b]; c = Cm z (Cm = E^-1 - I, kd^2 x kd^2 row-major); then
-// P = U C with C[i][j] = c[i*kd + j]  (D x kd)
+// z = sum_b partial[b]; mode 0: zc = z; mode 1: zc = Cm z (Cm = E^-1,
+// kd^2 x kd^2 row-major).  zc[i*kd + j] is the coefficient of u_i u_j^H.
 __global__ void k_defl_coef(const double2 *__restrict__ partial, int nb, const double2 *__restrict__ Cm,
                             int kd, double2 *__restrict__ zc, int mode) {
   __shared__ double2 z[KDMAX * KDMAX];
@@ -218,7 +280,7 @@ __global__ void k_defl_coef(const double2 *__restrict__ partial, int nb, const d
   }
 }
 
-// out[r,c] = in[r,c] + sum_{i,j} U[r,i] C[i,j] conj(U[c,j])
+// out[r,c] = in[r,c] + sum_{i,j} U[r,i] C[i,j] conj(U[c,j])   (in == nullptr: 0)
 __global__ void k_defl_expand(const double2 *__restrict__ in, double2 *__restrict__ out,
                               const double2 *__restrict__ U, const double2 *__restrict__ cvec, int D, int kd) {
   __shared__ double2 C[KDMAX * KDMAX];
@@ -244,7 +306,7 @@ __global__ void k_defl_expand(const double2 *__restrict__ in, double2 *__restric
   }
   for (int cc = 0; cc < DC && c0 + cc < D; cc++) {
     const size_t e = (size_t)(c0 + cc) * D + r;
-    double2 v = in[e];
+    double2 v = in ? in[e] : make_double2(0.0, 0.0);
     for (int j = 0; j < kd; j++) {
       const double2 t = cmuls(P[j], Uc[cc][j]);
       v.x += t.x; v.y += t.y;
@@ -268,31 +330,46 @@ int grid_for(int64_t n) {
 
 }  // namespace
 
-// GMRES state bound to one qsystem (buffers reused across solves).
+// GMRES state bound to one device (buffers reused across solves).  The
+// basis V holds complex128 or, in the FP32-inner solver, complex64 vectors;
+// the residual t and the work vector w are always complex128.
 struct Gmres {
-  int m = 0;
+  int m = 0, f32 = 0;
   int64_t n = 0;
-  double2 *V = nullptr;        // (m+1) x n
+  void *V = nullptr;           // (m+1) x n basis vectors
+  double2 *t = nullptr;        // residual / conversion buffer
   double2 *w = nullptr;
   double2 *partial = nullptr;  // (m+1) x nb
-  double2 *h = nullptr;        // m+1 projections
-  double2 *hh = nullptr;       // pinned host copy
+  double2 *h = nullptr;        // m+2: projections, then the norm
+  double2 *h2 = nullptr;       // second-pass projections
+  double *npart = nullptr;     // per-block partial norms
+  double2 *hh = nullptr;       // pinned host copy of h
   int nb = 0;
-  void ensure(int64_t n_, int m_) {
-    if (n_ == n && m_ == m) return;
+  template <typename VT> VT *basis() const { return static_cast<VT *>(V); }
+  void ensure(int64_t n_, int m_, int f32_) {
+    if (n_ == n && m_ == m && f32_ == f32) return;
     release();
     n = n_;
     m = m_;
+    f32 = f32_;
     nb = (int)((n + CHUNK - 1) / CHUNK);
-    QCUDA(cudaMalloc(&V, (size_t)(m + 1) * n * sizeof(double2)));
+    QCUDA(cudaMalloc(&V, (size_t)(m + 1) * n * (f32 ? sizeof(float2) : sizeof(double2))));
+    QCUDA(cudaMalloc(&t, (size_t)n * sizeof(double2)));
     QCUDA(cudaMalloc(&w, (size_t)n * sizeof(double2)));
     QCUDA(cudaMalloc(&partial, (size_t)(m + 1) * nb * sizeof(double2)));
-    QCUDA(cudaMalloc(&h, (size_t)(m + 1) * sizeof(double2)));
-    QCUDA(cudaMallocHost(&hh, (size_t)(m + 1) * sizeof(double2)));
+    QCUDA(cudaMalloc(&h, (size_t)(m + 2) * sizeof(double2)));
+    QCUDA(cudaMalloc(&h2, (size_t)(m + 1) * sizeof(double2)));
+    QCUDA(cudaMalloc(&npart, (size_t)grid_for(n) * sizeof(double)));
+    QCUDA(cudaMallocHost(&hh, (size_t)(m + 2) * sizeof(double2)));
   }
   void release() {
-    if (V) { cudaFree(V); cudaFree(w); cudaFree(partial); cudaFree(h); cudaFreeHost(hh); }
-    V = w = partial = h = hh = nullptr;
+    if (V) {
+      cudaFree(V); cudaFree(t); cudaFree(w); cudaFree(partial); cudaFree(h); cudaFree(h2); cudaFree(npart);
+      cudaFreeHost(hh);
+    }
+    V = nullptr;
+    t = w = partial = h = h2 = hh = nullptr;
+    npart = nullptr;
     n = 0;
     m = 0;
   }
@@ -332,17 +409,21 @@ static double norm2(const double2 *x, int64_t n, cudaStream_t s) {
   return std::sqrt(std::max(0.0, vdot(x, x, n, s).real()));
 }
 
-// Deflation preconditioner M = I + W (E^-1 - I) W^H with W = { vec(u_i u_j^H) }
-// and E = W^H A W (kd^2 x kd^2): the components of the residual in span W are
-// solved for exactly, so restarted GMRES no longer stalls on the slow modes
-// that W captures.
+// Deflation by W = { vec(u_i u_j^H) } (Galerkin projection):
+//   E = W^H A W,  Q = W E^-1 W^H,  P = I - A Q.
+// GMRES runs on P A; the true residual of x + Q r + (I - Q A) y is
+// P (r - A y), which is what the Arnoldi process minimises, so the components
+// of the residual in A span W are removed exactly and restarted GMRES no
+// longer stalls on the slow modes that W captures.  Unlike the right
+// preconditioner I + W (E^-1 - I) W^H, the projected operator does not get
+// worse conditioned than A when W is far from an invariant subspace.
 struct Deflation {
   int D = 0, kd = 0, nbx = 0, nby = 0;
-  double2 *U = nullptr, *Cm = nullptr, *partial = nullptr, *coef = nullptr, *t1 = nullptr, *t2 = nullptr;
+  double2 *U = nullptr, *Ei = nullptr, *partial = nullptr, *coef = nullptr, *t1 = nullptr, *t2 = nullptr;
   void release() {
-    for (double2 *p : {U, Cm, partial, coef, t1, t2})
+    for (double2 *p : {U, Ei, partial, coef, t1, t2})
       if (p) cudaFree(p);
-    U = Cm = partial = coef = t1 = t2 = nullptr;
+    U = Ei = partial = coef = t1 = t2 = nullptr;
   }
 };
 
@@ -354,10 +435,18 @@ static void defl_project(const Deflation &F, const double2 *in, const double2 *C
   count_launch(2);
 }
 
-// out = M in
-static void apply_M(const Deflation &F, const double2 *in, double2 *out, cudaStream_t s) {
-  defl_project(F, in, F.Cm, F.coef, 1, s);
-  k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(in, out, F.U, F.coef, F.D, F.kd);
+// out = Q in   (out may not alias in)
+static void apply_Q(const Deflation &F, const double2 *in, double2 *out, cudaStream_t s) {
+  defl_project(F, in, F.Ei, F.coef, 1, s);
+  k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, out, F.U, F.coef, F.D, F.kd);
+  count_launch();
+}
+
+// w <- P w = w - A Q w   (uses t1, t2)
+static void apply_P(const DeviceProgram &PP, const Deflation &F, double2 *w, int64_t n, cudaStream_t s) {
+  apply_Q(F, w, F.t1, s);
+  apply_A(PP, F.t1, F.t2, s);
+  k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(w, F.t2, n, -1.0);
   count_launch();
 }
 
@@ -399,96 +488,109 @@ static bool build_deflation(const DeviceProgram &PP, const std::complex<double> 
   F.nby = (D + DC - 1) / DC;
   const int K2 = kd * kd;
   QCUDA(cudaMalloc(&F.U, (size_t)D * kd * sizeof(double2)));
-  QCUDA(cudaMalloc(&F.Cm, (size_t)K2 * K2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.Ei, (size_t)K2 * K2 * sizeof(double2)));
   QCUDA(cudaMalloc(&F.partial, (size_t)F.nbx * F.nby * K2 * sizeof(double2)));
   QCUDA(cudaMalloc(&F.coef, (size_t)K2 * sizeof(double2)));
   QCUDA(cudaMalloc(&F.t1, n * sizeof(double2)));
   QCUDA(cudaMalloc(&F.t2, n * sizeof(double2)));
   if (has_error()) return false;
   QCUDA(cudaMemcpyAsync(F.U, U_host, (size_t)D * kd * sizeof(double2), cudaMemcpyHostToDevice, s));
-  // E[:, (k,l)] = W^H A vec(u_k u_l^H)
-  std::vector<std::complex<double>> E((size_t)K2 * K2);
-  std::vector<double2> unit(K2), col(K2);
+  // E[:, q] = W^H A vec(u_k u_l^H) for q = k*kd + l: every column is queued
+  // on the stream (unit coefficients from an identity block), one copy back
+  double2 *Id = nullptr, *Ecol = nullptr;
+  QCUDA(cudaMalloc(&Id, (size_t)K2 * K2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&Ecol, (size_t)K2 * K2 * sizeof(double2)));
+  if (has_error()) {
+    if (Id) cudaFree(Id);
+    if (Ecol) cudaFree(Ecol);
+    return false;
+  }
+  std::vector<double2> hId((size_t)K2 * K2, make_double2(0.0, 0.0)), hE((size_t)K2 * K2);
+  for (int q = 0; q < K2; q++) hId[(size_t)q * K2 + q] = make_double2(1.0, 0.0);
+  QCUDA(cudaMemcpyAsync(Id, hId.data(), hId.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
   for (int q = 0; q < K2; q++) {
-    for (int p = 0; p < K2; p++) unit[p] = make_double2(p == q ? 1.0 : 0.0, 0.0);
-    QCUDA(cudaMemcpyAsync(F.coef, unit.data(), K2 * sizeof(double2), cudaMemcpyHostToDevice, s));
-    QCUDA(cudaMemsetAsync(F.t1, 0, n * sizeof(double2), s));
-    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(F.t1, F.t1, F.U, F.coef, D, kd);
+    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, F.t1, F.U, Id + (size_t)q * K2, D, kd);
     count_launch();
     apply_A(PP, F.t1, F.t2, s);
-    defl_project(F, F.t2, nullptr, F.coef, 0, s);
-    QCUDA(cudaMemcpyAsync(col.data(), F.coef, K2 * sizeof(double2), cudaMemcpyDeviceToHost, s));
-    QCUDA(cudaStreamSynchronize(s));
-    for (int p = 0; p < K2; p++) E[(size_t)p * K2 + q] = std::complex<double>(col[p].x, col[p].y);
+    defl_project(F, F.t2, nullptr, Ecol + (size_t)q * K2, 0, s);
   }
+  QCUDA(cudaMemcpyAsync(hE.data(), Ecol, hE.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  QCUDA(cudaStreamSynchronize(s));
+  cudaFree(Id);
+  cudaFree(Ecol);
+  std::vector<std::complex<double>> E((size_t)K2 * K2);
+  for (int q = 0; q < K2; q++)
+    for (int p = 0; p < K2; p++) E[(size_t)p * K2 + q] = std::complex<double>(hE[(size_t)q * K2 + p].x, hE[(size_t)q * K2 + p].y);
   if (has_error() || !invert_small(E, K2)) return false;
-  std::vector<double2> Cm((size_t)K2 * K2);
-  for (int p = 0; p < K2; p++)
-    for (int q = 0; q < K2; q++) {
-      std::complex<double> v = E[(size_t)p * K2 + q] - (p == q ? 1.0 : 0.0);
-      Cm[(size_t)p * K2 + q] = make_double2(v.real(), v.imag());
-    }
-  QCUDA(cudaMemcpyAsync(F.Cm, Cm.data(), Cm.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+  std::vector<double2> Ei((size_t)K2 * K2);
+  for (size_t p = 0; p < Ei.size(); p++) Ei[p] = make_double2(E[p].real(), E[p].imag());
+  QCUDA(cudaMemcpyAsync(F.Ei, Ei.data(), Ei.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
   QCUDA(cudaStreamSynchronize(s));
   return !has_error();
 }
 
-// Returns iterations, fills x (device, length n).  rtol is relative to ||b|| = 1.
-int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, bool x_is_guess,
-                    double *final_res, const Deflation *def = nullptr) {
-  ensure_program(qs);
-  const DeviceProgram &PP = *qs->impl->prog;
-  const DevProg &P = PP.dev;
-  const int64_t n = (int64_t)P.D * P.ncols;
-  cudaStream_t s = stream_of(qs);
-  if (m < 1 || m > GMRES_MAXM) { fail(9, "ERROR! GMRES restart must be in [1, %d]\n", GMRES_MAXM); return -1; }
-  Gmres &G = gmres_for(qs);
-  G.ensure(n, m);
-  if (!x_is_guess) {
-    QCUDA(cudaMemsetAsync(x, 0, n * sizeof(double2), s));
-    const double2 one = make_double2(1.0, 0.0);
-    QCUDA(cudaMemcpyAsync(x, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
-  }
+// Restarted GMRES with the basis stored as VT.  Every restart forms the
+// true residual b - A x in complex128, so with a complex64 basis (FP32
+// inner) the restarts are the iterative refinement that takes the solution
+// to the complex128 tolerance.
+template <typename VT>
+static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double rtol, int m, int64_t maxit,
+                         double *final_res, const Deflation *def, cudaStream_t s) {
+  const int64_t n = G.n;
+  VT *V = G.basis<VT>();
   std::vector<std::complex<double>> H((size_t)(m + 1) * m), cs(m), sn(m), gvec(m + 1), y(m);
   int64_t it = 0;
   double res = 0;
   while (true) {
-    // r = b - A x  -> V_0
-    apply_A(PP, x, G.V, s);
-    k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.V, n);
+    // r = b - A x
+    apply_A(PP, x, G.t, s);
+    k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.t, n);
     count_launch();
-    const double beta = norm2(G.V, n, s);
+    double beta = norm2(G.t, n, s);
     res = beta;
     if (beta <= rtol || it >= maxit) break;
-    k_scale<<<grid_for(n), NT, 0, s>>>(G.V, G.V, n, 1.0 / beta);
+    if (def) {  // x += Q r, and the cycle starts from P r = r - A Q r
+      apply_Q(*def, G.t, def->t1, s);
+      k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, def->t1, n, 1.0);
+      apply_A(PP, def->t1, def->t2, s);
+      k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(G.t, def->t2, n, -1.0);
+      count_launch(2);
+      beta = norm2(G.t, n, s);
+      if (!(beta > rtol)) { it++; continue; }  // re-check the true residual
+    }
+    k_scale<<<grid_for(n), NT, 0, s>>>(G.t, V, n, 1.0 / beta);
     count_launch();
     std::fill(gvec.begin(), gvec.end(), 0.0);
     gvec[0] = beta;
     int j = 0;
-    bool conv = false;
     for (; j < m && it < maxit; j++, it++) {
-      if (def) {  // right preconditioning: Arnoldi on A M
-        apply_M(*def, G.V + (size_t)j * n, def->t1, s);
-        apply_A(PP, def->t1, G.w, s);
+      const VT *vj = V + (size_t)j * n;
+      if constexpr (std::is_same<VT, double2>::value) {
+        apply_A(PP, reinterpret_cast<const double2 *>(vj), G.w, s);
       } else {
-        apply_A(PP, G.V + (size_t)j * n, G.w, s);
+        k_scale<<<grid_for(n), NT, 0, s>>>(vj, G.t, n, 1.0);
+        count_launch();
+        apply_A(PP, G.t, G.w, s);
       }
-      // CGS2 with the projections summed on the host
-      std::vector<std::complex<double>> hsum(j + 1, 0.0);
-      for (int pass = 0; pass < 2; pass++) {
-        k_multidot<<<G.nb, NT, 0, s>>>(G.V, G.w, n, j + 1, G.partial);
-        k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, G.h, 0);
-        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j + 1, G.w, -1.0);
-        count_launch(3);
-        QCUDA(cudaMemcpyAsync(G.hh, G.h, (j + 1) * sizeof(double2), cudaMemcpyDeviceToHost, s));
-        QCUDA(cudaStreamSynchronize(s));
-        for (int k = 0; k <= j; k++) hsum[k] += std::complex<double>(G.hh[k].x, G.hh[k].y);
-      }
-      const double hn = norm2(G.w, n, s);
-      for (int k = 0; k <= j; k++) H[(size_t)k * m + j] = hsum[k];
+      if (def) apply_P(PP, *def, G.w, n, s);  // Arnoldi on P A
+      // CGS2 on the device; one copy of the Hessenberg column (projections
+      // of both passes summed, then ||w||) comes back per step
+      const dim3 gd(G.nb, (j + 1 + NT / 32 - 1) / (NT / 32));
+      k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial);
+      k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, G.h, 0);
+      k_multiaxpy<<<grid_for(n), NT, 0, s>>>(V, G.h, n, j + 1, G.w, -1.0);
+      k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial);
+      k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, G.h2, 0);
+      k_multiaxpy_norm<<<grid_for(n), NT, 0, s>>>(V, G.h2, n, j + 1, G.w, G.npart);
+      k_arnoldi_finish<<<1, NT, 0, s>>>(G.h, G.h2, j + 1, G.npart, grid_for(n));
+      count_launch(7);
+      QCUDA(cudaMemcpyAsync(G.hh, G.h, (j + 2) * sizeof(double2), cudaMemcpyDeviceToHost, s));
+      QCUDA(cudaStreamSynchronize(s));
+      const double hn = G.hh[j + 1].x;
+      for (int k = 0; k <= j; k++) H[(size_t)k * m + j] = std::complex<double>(G.hh[k].x, G.hh[k].y);
       H[(size_t)(j + 1) * m + j] = hn;
       if (hn > 0) {
-        k_scale<<<grid_for(n), NT, 0, s>>>(G.w, G.V + (size_t)(j + 1) * n, n, 1.0 / hn);
+        k_scale<<<grid_for(n), NT, 0, s>>>(G.w, V + (size_t)(j + 1) * n, n, 1.0 / hn);
         count_launch();
       }
       for (int k = 0; k < j; k++) {
@@ -504,7 +606,7 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
       H[(size_t)(j + 1) * m + j] = 0;
       gvec[j + 1] = -sn[j] * gvec[j];
       gvec[j] = std::conj(cs[j]) * gvec[j];
-      if (std::abs(gvec[j + 1]) <= rtol || hn == 0) { j++; it++; conv = true; break; }
+      if (std::abs(gvec[j + 1]) <= rtol || hn == 0) { j++; it++; break; }
     }
     // solve the triangular system and update x += V y
     for (int k = j - 1; k >= 0; k--) {
@@ -516,23 +618,48 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
       std::vector<double2> yh(j);
       for (int k = 0; k < j; k++) yh[k] = make_double2(y[k].real(), y[k].imag());
       QCUDA(cudaMemcpyAsync(G.h, yh.data(), j * sizeof(double2), cudaMemcpyHostToDevice, s));
-      if (def) {  // x += M (V y)
-        QCUDA(cudaMemsetAsync(def->t1, 0, n * sizeof(double2), s));
-        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j, def->t1, 1.0);
-        apply_M(*def, def->t1, def->t2, s);
-        k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, def->t2, n, 1.0);
+      if (def) {  // x += (I - Q A) V y
+        QCUDA(cudaMemsetAsync(G.w, 0, n * sizeof(double2), s));
+        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(V, G.h, n, j, G.w, 1.0);
+        k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, G.w, n, 1.0);
         count_launch(2);
+        apply_A(PP, G.w, def->t2, s);
+        apply_Q(*def, def->t2, def->t1, s);
+        k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, def->t1, n, -1.0);
+        count_launch();
       } else {
-        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(G.V, G.h, n, j, x, 1.0);
+        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(V, G.h, n, j, x, 1.0);
         count_launch();
       }
       QCUDA(cudaStreamSynchronize(s));
     }
-    (void)conv;
   }
   QCUDA(cudaStreamSynchronize(s));
   if (final_res) *final_res = res;
   return it;
+}
+
+// Returns iterations, fills x (device, length n).  rtol is relative to ||b|| = 1.
+// The basis precision follows quac_set_gmres_precision.
+int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, bool x_is_guess,
+                    double *final_res, const Deflation *def = nullptr) {
+  ensure_program(qs);
+  const DeviceProgram &PP = *qs->impl->prog;
+  const DevProg &P = PP.dev;
+  const int64_t n = (int64_t)P.D * P.ncols;
+  cudaStream_t s = stream_of(qs);
+  if (m < 1 || m > GMRES_MAXM) { fail(9, "ERROR! GMRES restart must be in [1, %d]\n", GMRES_MAXM); return -1; }
+  Gmres &G = gmres_for(qs);
+  const int f32 = options().gmres_f32;
+  G.ensure(n, m, f32);
+  if (has_error()) return -1;
+  if (!x_is_guess) {
+    QCUDA(cudaMemsetAsync(x, 0, n * sizeof(double2), s));
+    const double2 one = make_double2(1.0, 0.0);
+    QCUDA(cudaMemcpyAsync(x, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
+  }
+  return f32 ? gmres_run<float2>(PP, G, x, rtol, m, maxit, final_res, def, s)
+             : gmres_run<double2>(PP, G, x, rtol, m, maxit, final_res, def, s);
 }
 
 }  // namespace quac
@@ -576,19 +703,19 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
   {
     Gmres &G = gmres_for(qs);
     const int64_t n = (int64_t)PP.dev.D * PP.dev.D;
-    G.ensure(n, options().gmres_restart);
+    G.ensure(n, options().gmres_restart, options().gmres_f32);
     apply_A(PP, x->data->d, G.w, s);
     k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.w, n);
     count_launch();
     const double r_guess = norm2(G.w, n, s);
-    QCUDA(cudaMemsetAsync(G.V, 0, n * sizeof(double2), s));
+    QCUDA(cudaMemsetAsync(G.t, 0, n * sizeof(double2), s));
     const double2 one = make_double2(1.0, 0.0);
-    QCUDA(cudaMemcpyAsync(G.V, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
-    apply_A(PP, G.V, G.w, s);
+    QCUDA(cudaMemcpyAsync(G.t, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
+    apply_A(PP, G.t, G.w, s);
     k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.w, n);
     count_launch();
     const double r_e0 = norm2(G.w, n, s);
-    if (!(r_guess <= r_e0)) QCUDA(cudaMemcpyAsync(x->data->d, G.V, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    if (!(r_guess <= r_e0)) QCUDA(cudaMemcpyAsync(x->data->d, G.t, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
   }
   double res = 0;
   const int m = options().gmres_restart;

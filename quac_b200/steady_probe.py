@@ -1,0 +1,97 @@
+"""Steady states of a driven Tavis-Cummings sweep: learned warm start
+against cold GMRES on held-out parameter points.
+
+    python -m quac_b200.steady_probe [--ne 3] [--nc 4] [--train 48] [--held 12]
+                                     [--sweep2d] [--steps 8000] [--fp32 1] [--kd 8]
+
+Training states are generated by the solver itself (warmstart.generate),
+the network is trained on the GPU, then every held-out point is solved
+three ways, each to ||(L + e0 vec(I)^T) x - e0|| <= 1e-11:
+  cold     plain complex128 GMRES(100) from e0 (steady_state_sys);
+  method   the same solver setting as `learned` (basis precision per
+           --fp32) from e0 with no proposal: the method without the network;
+  learned  the network's proposal (initial state and deflation space) and
+           the solver setting per --fp32.
+Prints one JSON line: solves/s of each, the ratios, iteration counts and
+the largest population difference against the cold solve.
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import warmstart as WS
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ne", type=int, default=3)
+    ap.add_argument("--nc", type=int, default=4)
+    ap.add_argument("--train", type=int, default=48)
+    ap.add_argument("--held", type=int, default=12)
+    ap.add_argument("--sweep2d", action="store_true", help="kappa = 0.1 and gamma = 5e-3 fixed")
+    ap.add_argument("--steps", type=int, default=8000)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--fp32", type=int, default=1)
+    ap.add_argument("--kd", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=5)
+    a = ap.parse_args()
+    import quac_b200 as q
+    q.QuaC_initialize()
+
+    D = 2 ** a.ne * a.nc
+    fixed = {2: 0.1, 3: 5e-3} if a.sweep2d else None
+    thetas = WS.sweep_params(a.train + a.held, seed=a.seed, fixed=fixed)
+    train, held = thetas[:a.train], thetas[a.train:]
+    net = q.WarmStartNet(D, rank=16, hidden=256, batch=min(128, a.train), max_samples=a.train, seed=2)
+    q.set_gmres_precision(a.fp32)
+    t = time.perf_counter()
+    gen_its = WS.generate(q, net, train, a.ne, a.nc, kd=a.kd)
+    t_gen = time.perf_counter() - t
+    t = time.perf_counter()
+    loss = net.train(a.steps, lr=a.lr, seed=3)
+    t_train = time.perf_counter() - t
+
+    rows = []
+    for th in held:
+        q.set_gmres_precision(0)
+        xc, its_c, dt_c = WS.solve_cold(q, th, a.ne, a.nc)
+        q.set_gmres_precision(a.fp32)
+        xm, its_m, dt_m = WS.solve_cold(q, th, a.ne, a.nc)
+        t = time.perf_counter()
+        x0, U = WS.proposal_from_factors(net.predict(WS.normalize(th)[None, :])[0], a.kd)
+        dt_p = time.perf_counter() - t
+        B, v, its_l, res, dt_s = WS.solve_guided(q, th, a.ne, a.nc, x0, U)
+        xl = v.to_numpy()
+        v.destroy()
+        B.qs.destroy()
+        dt_l = dt_p + dt_s  # network inference + proposal + solve
+        pc = xc.reshape(D, D, order="F").diagonal().real
+        perr = max(np.abs(x.reshape(D, D, order="F").diagonal().real - pc).max() for x in (xm, xl))
+        rows.append((its_c, dt_c, its_m, dt_m, its_l, dt_l, perr, res))
+    q.set_gmres_precision(0)
+    r = np.array(rows)
+    n = len(held)
+    out = {
+        "workload": f"tavis_cummings_steady_ne{a.ne}_nc{a.nc}_D{D}",
+        "sweep": "2d (omega, delta)" if a.sweep2d else "4d (omega, delta, kappa, gamma)",
+        "train_states": a.train, "held_out": n, "kd": a.kd,
+        "solver": "fp32-inner/fp64-refined" if a.fp32 else "fp64",
+        "generation": {"seconds": t_gen, "mean_iterations": float(np.mean(gen_its))},
+        "training": {"steps": a.steps, "seconds": t_train, "loss": loss},
+        "cold": {"solves_per_s": n / r[:, 1].sum(), "iterations": r[:, 0].astype(int).tolist()},
+        "method": {"solves_per_s": n / r[:, 3].sum(), "iterations": r[:, 2].astype(int).tolist()},
+        "learned": {"solves_per_s": n / r[:, 5].sum(), "iterations": r[:, 4].astype(int).tolist()},
+        "learned_vs_cold": r[:, 1].sum() / r[:, 5].sum(),
+        "learned_vs_method": r[:, 3].sum() / r[:, 5].sum(),
+        "method_vs_cold": r[:, 1].sum() / r[:, 3].sum(),
+        "pop_err_max": float(r[:, 6].max()),
+        "residual_max": float(r[:, 7].max()),
+    }
+    net.destroy()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -114,6 +114,54 @@ def test_guided_steady_state_falls_back_to_plain_gmres(quac, oracle):
     B.qs.destroy()
 
 
+def _residual(oracle, ne, nc, p, x):
+    import scipy.sparse as sp
+    O = oracle.OSys()
+    Sy.tavis_cummings(O, ne=ne, nc=nc, g=0.1, **p)
+    L = O.liouvillian().tocsr()
+    n = L.shape[0]
+    D = int(round(np.sqrt(n)))
+    row = sp.csr_matrix((np.eye(D).reshape(-1, order="F"), (np.zeros(n, int), np.arange(n))), shape=(n, n))
+    b = np.zeros(n, complex)
+    b[0] = 1
+    return np.linalg.norm((L + row) @ x - b)
+
+
+@pytest.mark.parametrize("guided", [False, True], ids=["cold", "guided"])
+def test_fp32_inner_gmres_reaches_fp64_tolerance(quac, oracle, guided):
+    """complex64 Krylov basis, complex128 residual at every restart: the
+    answer meets the same complex128 residual bar as the plain solver."""
+    ne, nc = 3, 4
+    xs, D = _oracle_steady(oracle, ne, nc, TC_POINT)
+    B = Sy.Builder(quac)
+    Sy.tavis_cummings(B, ne=ne, nc=nc, g=0.1, **TC_POINT)
+    quac.construct_matrix(B.qs)
+    g = quac.create_qvec_sys(B.qs)
+    quac.set_gmres_precision(1)
+    try:
+        if guided:
+            U, w = _factors(xs, D, 16)
+            x0 = (U * np.maximum(w, 0)) @ U.conj().T
+            g.from_numpy((x0 / np.trace(x0)).reshape(-1, order="F"))
+            its, res = quac.steady_state_guided(B.qs, g, U[:, :8])
+            assert res <= 1e-11
+        else:
+            its = quac.steady_state_sys(B.qs, g)
+    finally:
+        quac.set_gmres_precision(0)
+    y = g.to_numpy()
+    r = _residual(oracle, ne, nc, TC_POINT, y)
+    print(f"fp32-inner {'guided' if guided else 'cold'}: {its} iterations, residual {r:.2e}")
+    assert r <= 2e-11
+    assert np.linalg.norm(y - xs) / np.linalg.norm(xs) < 1e-8
+    pops = y.reshape(D, D, order="F").diagonal().real
+    assert np.abs(pops - xs.reshape(D, D, order="F").diagonal().real).max() < 1e-8
+    with pytest.raises(quac.QuacError):
+        quac.set_gmres_precision(2)
+    g.destroy()
+    B.qs.destroy()
+
+
 # ------------------------------------------------------------ network kernels
 def _random_states(rng, n, D):
     out = []

@@ -303,12 +303,19 @@ int quac_ensemble_populations(quac_ensemble ens, double *pops);
 /* Steady state from a proposed initial state and a proposed dominant
  * subspace (no reference counterpart; solver.c:33-221 always starts from
  * e0).  x holds the initial guess on entry.  U: D x kd column-major, with
- * orthonormal columns (kd <= 8); the kd^2 matrices u_i u_j^H span the
- * deflation space of the preconditioner.  The solve starts from x or e0,
- * whichever has the smaller residual; deflated GMRES(100) runs for at most
- * maxit_guided iterations, then plain GMRES(100) continues from its
- * iterate if needed.  Same system and tolerance as steady_state.  Returns
- * the iterations (-1 on error); *residual = ||b - A x|| at the end. */
+ * orthonormal columns (kd <= 16); the kd^2 matrices u_i u_j^H span the
+ * deflation space W.  GMRES runs on P A with P = I - A W (W^H A W)^-1 W^H
+ * (Galerkin projection) and the iterate is corrected after each restart,
+ * so the residual components in A span W are removed exactly.  With
+ * deflation refresh on (default), every restart after the first replaces
+ * U by one Rayleigh-Ritz step toward the kd leading eigenvectors of the
+ * Hermitian part of the current iterate.  The solve starts from x or e0,
+ * whichever has the smaller residual; deflated GMRES runs for at most
+ * maxit_guided iterations, then plain GMRES continues from its iterate if
+ * needed (restart length per quac_set_gmres_restart, basis precision per
+ * quac_set_gmres_precision).  Same system and tolerance as steady_state.
+ * Returns the iterations (-1 on error); *residual = ||b - A x|| at the
+ * end. */
 PetscInt quac_steady_state_guided(qsystem qsys, qvec x, const PetscScalar *U, PetscInt kd,
                                   PetscInt maxit_guided, PetscReal *residual);
 /* Learned warm start for steady states (no reference counterpart): an MLP
@@ -380,6 +387,12 @@ int quac_set_gmres_restart(int m);
  * complex128, so each restart refines the solution to the same
  * complex128 tolerance. */
 int quac_set_gmres_precision(int precision);
+/* Deflation refresh of quac_steady_state_guided (no reference
+ * counterpart): 1 (default) = at every restart after the first, the
+ * deflation space is rebuilt from one Rayleigh-Ritz step toward the
+ * leading eigenvectors of the current iterate; 0 = the proposed U is kept
+ * for the whole solve. */
+int quac_set_deflation_refresh(int mode);
 /* Number of L.x applications that ran in Hermitian mode (diagnostics). */
 int64_t quac_hermitian_apply_count(void);
 /* Number of kernels this library has launched (diagnostics). */

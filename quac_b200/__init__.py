@@ -169,6 +169,7 @@ def lib():
         "quac_set_hermitian_mode": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_restart": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_precision": (ctypes.c_int, [ctypes.c_int]),
+        "quac_set_deflation_refresh": (ctypes.c_int, [ctypes.c_int]),
         "quac_hermitian_apply_count": (i64, []),
         "VecGetSize": (ctypes.c_int, [vp, P(i64)]),
         "read_qvec_dm_binary": (None, [P(P(_QvecStruct)), ctypes.c_char_p]),
@@ -688,6 +689,13 @@ def set_gmres_precision(precision):
     """0 (default): complex128 GMRES basis; 1: complex64 basis (FP32 inner),
     complex128 residual and iterate at every restart (FP64 refined)."""
     lib().quac_set_gmres_precision(int(precision))
+    _check()
+
+
+def set_deflation_refresh(mode):
+    """1 (default): steady_state_guided rebuilds its deflation space from the
+    iterate at every restart; 0: keeps the proposed one."""
+    lib().quac_set_deflation_refresh(int(mode))
     _check()
 
 

@@ -1194,6 +1194,12 @@ extern "C" int quac_set_gmres_precision(int precision) {
   return 0;
 }
 
+extern "C" int quac_set_deflation_refresh(int mode) {
+  if (mode != 0 && mode != 1) { fail(0, "ERROR! deflation refresh must be 0 (off) or 1 (every restart)\n"); return 1; }
+  options().defl_refresh = mode;
+  return 0;
+}
+
 extern "C" int quac_set_hermitian_mode(int mode) {
   if (mode != 0 && mode != 1) { fail(0, "ERROR! Hermitian mode must be 0 (off) or 1 (automatic)\n"); return 1; }
   options().herm_mode = mode;

@@ -39,6 +39,7 @@ struct Options {
   int lrho_f32 = 0;                 // see quac_set_lrho_precision
   int herm_mode = 1;                // see quac_set_hermitian_mode
   int gmres_f32 = 0;                // see quac_set_gmres_precision
+  int defl_refresh = 1;             // see quac_set_deflation_refresh
   int gmres_restart = 100;          // -ksp_gmres_restart (solver.c uses PETSc's default 100 via KSPGMRESSetRestart)
   bool rk4_classic = false;         // rk_type "4classic": four-stage form instead of Horner
 };

@@ -7,6 +7,7 @@
 // (m+1) x n block so the Gram-Schmidt projections are two streaming
 // kernels per pass (multi-dot, multi-axpy), repeated once (CGS2).  Only the
 // (m+1) x m Hessenberg matrix lives on the host.
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <memory>
@@ -207,7 +208,7 @@ __global__ void k_e0_minus(double2 *__restrict__ r, int64_t n) {
 // W = { vec(u_i u_j^H) } (kd^2 orthonormal vectors); W^H x = U^H X U.
 constexpr int DR = 128;  // rows per block
 constexpr int DC = 32;   // columns per block
-constexpr int KDMAX = 8;
+constexpr int KDMAX = 16;
 
 // partial[b][i*kd + j] = sum over this block's rows r and columns c of conj(U[r,i]) X[r,c] U[c,j]
 __global__ void k_defl_proj(const double2 *__restrict__ X, const double2 *__restrict__ U, int D, int kd,
@@ -225,10 +226,13 @@ __global__ void k_defl_proj(const double2 *__restrict__ X, const double2 *__rest
   if (r < D) {
     for (int cc = 0; cc < DC && c0 + cc < D; cc++) {
       const double2 x = X[(size_t)(c0 + cc) * D + r];
-      for (int j = 0; j < kd; j++) {
-        const double2 u = Uc[cc][j];
-        T[j].x = fma(x.x, u.x, fma(-x.y, u.y, T[j].x));
-        T[j].y = fma(x.x, u.y, fma(x.y, u.x, T[j].y));
+#pragma unroll
+      for (int j = 0; j < KDMAX; j++) {
+        if (j < kd) {
+          const double2 u = Uc[cc][j];
+          T[j].x = fma(x.x, u.x, fma(-x.y, u.y, T[j].x));
+          T[j].y = fma(x.x, u.y, fma(x.y, u.x, T[j].y));
+        }
       }
     }
   }
@@ -236,13 +240,16 @@ __global__ void k_defl_proj(const double2 *__restrict__ X, const double2 *__rest
   for (int i = 0; i < kd; i++) {
     double2 ui = (r < D) ? U[(size_t)i * D + r] : make_double2(0.0, 0.0);
     ui.y = -ui.y;
-    for (int j = 0; j < kd; j++) {
-      double2 p = cmuls(ui, T[j]);
-      for (int o = 16; o > 0; o >>= 1) {
-        p.x += __shfl_down_sync(0xffffffffu, p.x, o);
-        p.y += __shfl_down_sync(0xffffffffu, p.y, o);
+#pragma unroll
+    for (int j = 0; j < KDMAX; j++) {
+      if (j < kd) {
+        double2 p = cmuls(ui, T[j]);
+        for (int o = 16; o > 0; o >>= 1) {
+          p.x += __shfl_down_sync(0xffffffffu, p.x, o);
+          p.y += __shfl_down_sync(0xffffffffu, p.y, o);
+        }
+        if (lane == 0) red[w][i * kd + j] = p;
       }
-      if (lane == 0) red[w][i * kd + j] = p;
     }
   }
   __syncthreads();
@@ -296,26 +303,104 @@ __global__ void k_defl_expand(const double2 *__restrict__ in, double2 *__restric
   __syncthreads();
   if (r >= D) return;
   double2 P[KDMAX];
-  for (int j = 0; j < kd; j++) {
+#pragma unroll
+  for (int j = 0; j < KDMAX; j++) {
     double2 acc = make_double2(0.0, 0.0);
-    for (int i = 0; i < kd; i++) {
-      const double2 t = cmuls(U[(size_t)i * D + r], C[i * kd + j]);
-      acc.x += t.x; acc.y += t.y;
+    if (j < kd) {
+      for (int i = 0; i < kd; i++) {
+        const double2 t = cmuls(U[(size_t)i * D + r], C[i * kd + j]);
+        acc.x += t.x; acc.y += t.y;
+      }
     }
     P[j] = acc;
   }
   for (int cc = 0; cc < DC && c0 + cc < D; cc++) {
     const size_t e = (size_t)(c0 + cc) * D + r;
     double2 v = in ? in[e] : make_double2(0.0, 0.0);
-    for (int j = 0; j < kd; j++) {
-      const double2 t = cmuls(P[j], Uc[cc][j]);
-      v.x += t.x; v.y += t.y;
+#pragma unroll
+    for (int j = 0; j < KDMAX; j++) {
+      if (j < kd) {
+        const double2 t = cmuls(P[j], Uc[cc][j]);
+        v.x += t.x; v.y += t.y;
+      }
     }
     out[e] = v;
   }
 }
 
-// y = x + a * y  (a real)
+// Y += (X Z) / 2 for X (D x D) and Z (D x k, k <= KDMAX), both column-major:
+// thread = row r, block column = a segment of XSEG columns of X, segments
+// summed with atomics (Y zeroed by the caller).
+constexpr int XSEG = 64;
+__global__ void k_x_mul(const double2 *__restrict__ X, const double2 *__restrict__ Z, int D, int k,
+                        double2 *__restrict__ Y) {
+  __shared__ double2 Zs[XSEG][KDMAX];
+  const int r = blockIdx.x * DR + threadIdx.x, c0 = blockIdx.y * XSEG;
+  for (int q = threadIdx.x; q < XSEG * k; q += DR) {
+    const int cc = q / k, i = q % k;
+    Zs[cc][i] = (c0 + cc < D) ? Z[(size_t)i * D + c0 + cc] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  if (r >= D) return;
+  double2 acc[KDMAX];
+#pragma unroll
+  for (int i = 0; i < KDMAX; i++) acc[i] = make_double2(0.0, 0.0);
+  const int cend = min(XSEG, D - c0);
+  for (int cc = 0; cc < cend; cc++) {
+    const double2 xv = X[(size_t)(c0 + cc) * D + r];
+#pragma unroll
+    for (int i = 0; i < KDMAX; i++) {
+      if (i < k) {
+        const double2 t = cmuls(xv, Zs[cc][i]);
+        acc[i].x += t.x; acc[i].y += t.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < KDMAX; i++) {
+    if (i < k) {
+      atomicAdd(&Y[(size_t)i * D + r].x, 0.5 * acc[i].x);
+      atomicAdd(&Y[(size_t)i * D + r].y, 0.5 * acc[i].y);
+    }
+  }
+}
+
+// Y += (X^H Z) / 2: one warp per row r of the result, reading column r of X.
+__global__ void k_xh_mul(const double2 *__restrict__ X, const double2 *__restrict__ Z, int D, int k,
+                         double2 *__restrict__ Y) {
+  const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (r >= D) return;  // uniform across the warp
+  double2 acc[KDMAX];
+#pragma unroll
+  for (int i = 0; i < KDMAX; i++) acc[i] = make_double2(0.0, 0.0);
+  for (int c = lane; c < D; c += 32) {
+    double2 xv = X[(size_t)r * D + c];
+    xv.y = -xv.y;
+#pragma unroll
+    for (int i = 0; i < KDMAX; i++) {
+      if (i < k) {
+        const double2 t = cmuls(xv, Z[(size_t)i * D + c]);
+        acc[i].x += t.x; acc[i].y += t.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < KDMAX; i++) {
+    if (i < k) {
+      double2 v = acc[i];
+      for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&Y[(size_t)i * D + r].x, 0.5 * v.x);
+        atomicAdd(&Y[(size_t)i * D + r].y, 0.5 * v.y);
+      }
+    }
+  }
+}
+
+// y += a * x  (a real)
 __global__ void k_axpy_inplace(double2 *__restrict__ y, const double2 *__restrict__ x, int64_t n, double a) {
   for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
     const double2 v = x[i], w = y[i];
@@ -420,10 +505,13 @@ static double norm2(const double2 *x, int64_t n, cudaStream_t s) {
 struct Deflation {
   int D = 0, kd = 0, nbx = 0, nby = 0;
   double2 *U = nullptr, *Ei = nullptr, *partial = nullptr, *coef = nullptr, *t1 = nullptr, *t2 = nullptr;
+  double2 *Y = nullptr, *Z = nullptr;    // D x KDMAX each (subspace refresh)
+  double2 *Id = nullptr, *Ecol = nullptr;  // kd^2 x kd^2 each (assembly of E)
+  std::vector<std::complex<double>> Uh;  // host copy of U, column-major D x kd
   void release() {
-    for (double2 *p : {U, Ei, partial, coef, t1, t2})
+    for (double2 *p : {U, Ei, partial, coef, t1, t2, Y, Z, Id, Ecol})
       if (p) cudaFree(p);
-    U = Ei = partial = coef = t1 = t2 = nullptr;
+    U = Ei = partial = coef = t1 = t2 = Y = Z = Id = Ecol = nullptr;
   }
 };
 
@@ -477,9 +565,54 @@ static bool invert_small(std::vector<std::complex<double>> &A, int n) {
   return true;
 }
 
-// Builds the deflation preconditioner from host U (D x kd, column-major).
-static bool build_deflation(const DeviceProgram &PP, const std::complex<double> *U_host, int kd, Deflation &F,
-                            cudaStream_t s) {
+// Eigen-decomposition of a Hermitian n x n matrix (row-major; A is
+// overwritten): cyclic Jacobi.  Each rotation first scales row and column q
+// by a phase so that A[p][q] is real, then applies the real Jacobi rotation
+// of the symmetric 2 x 2 problem (Rutishauser's form: t = sgn(th) /
+// (|th| + sqrt(th^2 + 1)), th = (a_qq - a_pp) / (2 a_pq)).  Returns the
+// eigenvalues in w and the eigenvectors as the columns of V (row-major).
+static void herm_eig(std::vector<cplx> &A, int n, std::vector<double> &w, std::vector<cplx> &V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 60; sweep++) {
+    double off = 0.0, diag = 0.0;
+    for (int p = 0; p < n; p++)
+      for (int q = 0; q < n; q++) (p == q ? diag : off) += std::norm(A[(size_t)p * n + q]);
+    if (off <= 1e-30 * (diag + off)) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        const cplx apq = A[(size_t)p * n + q];
+        const double r = std::abs(apq);
+        if (r <= 1e-300) continue;
+        const cplx ph = apq / r, cph = std::conj(ph);
+        for (int k = 0; k < n; k++) A[(size_t)k * n + q] *= cph;
+        for (int k = 0; k < n; k++) A[(size_t)q * n + k] *= ph;
+        for (int k = 0; k < n; k++) V[(size_t)k * n + q] *= cph;
+        const double th = (A[(size_t)q * n + q].real() - A[(size_t)p * n + p].real()) / (2.0 * r);
+        const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < n; k++) {
+          const cplx a = A[(size_t)k * n + p], b = A[(size_t)k * n + q];
+          A[(size_t)k * n + p] = c * a - sn * b;
+          A[(size_t)k * n + q] = sn * a + c * b;
+        }
+        for (int k = 0; k < n; k++) {
+          const cplx a = A[(size_t)p * n + k], b = A[(size_t)q * n + k];
+          A[(size_t)p * n + k] = c * a - sn * b;
+          A[(size_t)q * n + k] = sn * a + c * b;
+        }
+        for (int k = 0; k < n; k++) {
+          const cplx a = V[(size_t)k * n + p], b = V[(size_t)k * n + q];
+          V[(size_t)k * n + p] = c * a - sn * b;
+          V[(size_t)k * n + q] = sn * a + c * b;
+        }
+      }
+  }
+  w.resize(n);
+  for (int i = 0; i < n; i++) w[i] = A[(size_t)i * n + i].real();
+}
+
+static bool alloc_deflation(const DeviceProgram &PP, int kd, Deflation &F) {
   const int D = PP.dev.D;
   const int64_t n = (int64_t)D * D;
   F.D = D;
@@ -493,39 +626,178 @@ static bool build_deflation(const DeviceProgram &PP, const std::complex<double> 
   QCUDA(cudaMalloc(&F.coef, (size_t)K2 * sizeof(double2)));
   QCUDA(cudaMalloc(&F.t1, n * sizeof(double2)));
   QCUDA(cudaMalloc(&F.t2, n * sizeof(double2)));
-  if (has_error()) return false;
-  QCUDA(cudaMemcpyAsync(F.U, U_host, (size_t)D * kd * sizeof(double2), cudaMemcpyHostToDevice, s));
-  // E[:, q] = W^H A vec(u_k u_l^H) for q = k*kd + l: every column is queued
-  // on the stream (unit coefficients from an identity block), one copy back
-  double2 *Id = nullptr, *Ecol = nullptr;
-  QCUDA(cudaMalloc(&Id, (size_t)K2 * K2 * sizeof(double2)));
-  QCUDA(cudaMalloc(&Ecol, (size_t)K2 * K2 * sizeof(double2)));
-  if (has_error()) {
-    if (Id) cudaFree(Id);
-    if (Ecol) cudaFree(Ecol);
-    return false;
-  }
+  QCUDA(cudaMalloc(&F.Y, (size_t)D * KDMAX * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.Z, (size_t)D * KDMAX * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.Id, (size_t)K2 * K2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&F.Ecol, (size_t)K2 * K2 * sizeof(double2)));
+  return !has_error();
+}
+
+// E = W^H A W for the U on the device and Ei = E^-1.  E[:, q] for
+// q = k*kd + l is W^H A vec(u_k u_l^H); every column is queued on the
+// stream (unit coefficients from an identity block), one copy back.
+// Returns false, leaving Ei as it was, if E is singular.
+static bool assemble_E(const DeviceProgram &PP, Deflation &F, cudaStream_t s) {
+  const int kd = F.kd, K2 = kd * kd;
   std::vector<double2> hId((size_t)K2 * K2, make_double2(0.0, 0.0)), hE((size_t)K2 * K2);
   for (int q = 0; q < K2; q++) hId[(size_t)q * K2 + q] = make_double2(1.0, 0.0);
-  QCUDA(cudaMemcpyAsync(Id, hId.data(), hId.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+  QCUDA(cudaMemcpyAsync(F.Id, hId.data(), hId.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
   for (int q = 0; q < K2; q++) {
-    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, F.t1, F.U, Id + (size_t)q * K2, D, kd);
+    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, F.t1, F.U, F.Id + (size_t)q * K2, F.D, kd);
     count_launch();
     apply_A(PP, F.t1, F.t2, s);
-    defl_project(F, F.t2, nullptr, Ecol + (size_t)q * K2, 0, s);
+    defl_project(F, F.t2, nullptr, F.Ecol + (size_t)q * K2, 0, s);
   }
-  QCUDA(cudaMemcpyAsync(hE.data(), Ecol, hE.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  QCUDA(cudaMemcpyAsync(hE.data(), F.Ecol, hE.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));
-  cudaFree(Id);
-  cudaFree(Ecol);
-  std::vector<std::complex<double>> E((size_t)K2 * K2);
+  std::vector<cplx> E((size_t)K2 * K2);
   for (int q = 0; q < K2; q++)
-    for (int p = 0; p < K2; p++) E[(size_t)p * K2 + q] = std::complex<double>(hE[(size_t)q * K2 + p].x, hE[(size_t)q * K2 + p].y);
+    for (int p = 0; p < K2; p++) E[(size_t)p * K2 + q] = cplx(hE[(size_t)q * K2 + p].x, hE[(size_t)q * K2 + p].y);
   if (has_error() || !invert_small(E, K2)) return false;
   std::vector<double2> Ei((size_t)K2 * K2);
   for (size_t p = 0; p < Ei.size(); p++) Ei[p] = make_double2(E[p].real(), E[p].imag());
   QCUDA(cudaMemcpyAsync(F.Ei, Ei.data(), Ei.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
   QCUDA(cudaStreamSynchronize(s));
+  return !has_error();
+}
+
+static void upload_U(Deflation &F, cudaStream_t s) {
+  std::vector<double2> h(F.Uh.size());
+  for (size_t i = 0; i < h.size(); i++) h[i] = make_double2(F.Uh[i].real(), F.Uh[i].imag());
+  QCUDA(cudaMemcpyAsync(F.U, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+  QCUDA(cudaStreamSynchronize(s));
+}
+
+// Builds the deflation from host U (D x kd, column-major, orthonormal columns).
+static bool build_deflation(const DeviceProgram &PP, const cplx *U_host, int kd, Deflation &F, cudaStream_t s) {
+  if (!alloc_deflation(PP, kd, F)) return false;
+  F.Uh.assign(U_host, U_host + (size_t)PP.dev.D * kd);
+  upload_U(F, s);
+  return assemble_E(PP, F, s);
+}
+
+// Y = Xh Z on the device for Xh = (X + X^H) / 2, Z (D x k) host, Y returned on the host.
+static std::vector<cplx> herm_part_times(const double2 *x, Deflation &F, const std::vector<cplx> &Zh, int k,
+                                         cudaStream_t s) {
+  const int D = F.D;
+  std::vector<double2> h((size_t)D * k);
+  for (size_t i = 0; i < h.size(); i++) h[i] = make_double2(Zh[i].real(), Zh[i].imag());
+  QCUDA(cudaMemcpyAsync(F.Z, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+  QCUDA(cudaMemsetAsync(F.Y, 0, (size_t)D * k * sizeof(double2), s));
+  k_x_mul<<<dim3((D + DR - 1) / DR, (D + XSEG - 1) / XSEG), DR, 0, s>>>(x, F.Z, D, k, F.Y);
+  k_xh_mul<<<(int)(((int64_t)D * 32 + NT - 1) / NT), NT, 0, s>>>(x, F.Z, D, k, F.Y);
+  count_launch(2);
+  QCUDA(cudaMemcpyAsync(h.data(), F.Y, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  QCUDA(cudaStreamSynchronize(s));
+  std::vector<cplx> Y(h.size());
+  for (size_t i = 0; i < h.size(); i++) Y[i] = cplx(h[i].x, h[i].y);
+  return Y;
+}
+
+// One Rayleigh-Ritz step toward the kd leading eigenvectors of the
+// Hermitian part Xh of the current iterate: the search space is span{U, Xh U}
+// (Xh U orthogonalised against U, directions below 1e-12 of the largest
+// dropped), the new U the kd Ritz vectors of Xh with the largest Ritz
+// values.  Warm-started from the previous U, one step per restart tracks
+// the iterate's dominant subspace as it converges.  E is then reassembled;
+// if that fails, the previous U and E are kept.
+static bool refresh_deflation(const DeviceProgram &PP, const double2 *x, Deflation &F, cudaStream_t s) {
+  const int D = F.D, kd = F.kd;
+  const std::vector<cplx> U = F.Uh;
+  auto col = [D](const std::vector<cplx> &M, int j) { return M.data() + (size_t)j * D; };
+  std::vector<cplx> Y = herm_part_times(x, F, U, kd, s);
+  if (has_error()) return false;
+  // Y <- Y - U (U^H Y)
+  for (int j = 0; j < kd; j++) {
+    cplx *y = Y.data() + (size_t)j * D;
+    for (int i = 0; i < kd; i++) {
+      const cplx *u = col(U, i);
+      cplx d = 0.0;
+      for (int r = 0; r < D; r++) d += std::conj(u[r]) * y[r];
+      for (int r = 0; r < D; r++) y[r] -= d * u[r];
+    }
+  }
+  // orthonormal basis of span Y from the eigenvectors of its Gram matrix
+  std::vector<cplx> G((size_t)kd * kd), Vg;
+  std::vector<double> g;
+  for (int i = 0; i < kd; i++)
+    for (int j = 0; j < kd; j++) {
+      cplx d = 0.0;
+      for (int r = 0; r < D; r++) d += std::conj(Y[(size_t)i * D + r]) * Y[(size_t)j * D + r];
+      G[(size_t)i * kd + j] = d;
+    }
+  herm_eig(G, kd, g, Vg);
+  double gmax = 0.0;
+  for (double v : g) gmax = std::max(gmax, v);
+  std::vector<cplx> Yo;
+  int k2 = 0;
+  for (int j = 0; j < kd; j++) {
+    if (!(g[j] > 1e-24 * gmax) || gmax <= 0.0) continue;
+    const double sc = 1.0 / std::sqrt(g[j]);
+    Yo.resize((size_t)(k2 + 1) * D, 0.0);
+    for (int i = 0; i < kd; i++) {
+      const cplx c = Vg[(size_t)i * kd + j] * sc;
+      for (int r = 0; r < D; r++) Yo[(size_t)k2 * D + r] += c * Y[(size_t)i * D + r];
+    }
+    k2++;
+  }
+  // Ritz problem on Z = [U, Yo]: T = Z^H Xh Z with Xh U = Y + U (U^H Xh U)
+  // recomputed from scratch for accuracy
+  const int nz = kd + k2;
+  std::vector<cplx> Z((size_t)nz * D);
+  std::copy(U.begin(), U.end(), Z.begin());
+  std::copy(Yo.begin(), Yo.end(), Z.begin() + (size_t)kd * D);
+  std::vector<cplx> XZ = herm_part_times(x, F, std::vector<cplx>(Z.begin(), Z.begin() + (size_t)kd * D), kd, s);
+  if (k2 > 0) {
+    std::vector<cplx> XY = herm_part_times(x, F, Yo, k2, s);
+    XZ.insert(XZ.end(), XY.begin(), XY.end());
+  }
+  if (has_error()) return false;
+  std::vector<cplx> T((size_t)nz * nz), Vt;
+  for (int i = 0; i < nz; i++)
+    for (int j = 0; j < nz; j++) {
+      cplx d = 0.0;
+      for (int r = 0; r < D; r++) d += std::conj(Z[(size_t)i * D + r]) * XZ[(size_t)j * D + r];
+      T[(size_t)i * nz + j] = d;
+    }
+  for (int i = 0; i < nz; i++)
+    for (int j = i; j < nz; j++) {
+      const cplx a = 0.5 * (T[(size_t)i * nz + j] + std::conj(T[(size_t)j * nz + i]));
+      T[(size_t)i * nz + j] = a;
+      T[(size_t)j * nz + i] = std::conj(a);
+    }
+  std::vector<double> w;
+  herm_eig(T, nz, w, Vt);
+  std::vector<int> order(nz);
+  for (int i = 0; i < nz; i++) order[i] = i;
+  std::sort(order.begin(), order.end(), [&w](int a, int b) { return w[a] > w[b]; });
+  std::vector<cplx> Un((size_t)kd * D, 0.0);
+  for (int j = 0; j < kd; j++) {
+    cplx *u = Un.data() + (size_t)j * D;
+    for (int i = 0; i < nz; i++) {
+      const cplx c = Vt[(size_t)i * nz + order[j]];
+      for (int r = 0; r < D; r++) u[r] += c * Z[(size_t)i * D + r];
+    }
+    // re-orthonormalise against the columns before it (modified Gram-Schmidt)
+    for (int i = 0; i < j; i++) {
+      const cplx *v = Un.data() + (size_t)i * D;
+      cplx d = 0.0;
+      for (int r = 0; r < D; r++) d += std::conj(v[r]) * u[r];
+      for (int r = 0; r < D; r++) u[r] -= d * v[r];
+    }
+    double nn = 0.0;
+    for (int r = 0; r < D; r++) nn += std::norm(u[r]);
+    if (!(nn > 0.0)) return false;
+    const double sc = 1.0 / std::sqrt(nn);
+    for (int r = 0; r < D; r++) u[r] *= sc;
+  }
+  F.Uh = Un;
+  upload_U(F, s);
+  if (!assemble_E(PP, F, s)) {
+    F.Uh = U;
+    upload_U(F, s);
+    return false;
+  }
   return !has_error();
 }
 
@@ -535,13 +807,14 @@ static bool build_deflation(const DeviceProgram &PP, const std::complex<double> 
 // to the complex128 tolerance.
 template <typename VT>
 static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double rtol, int m, int64_t maxit,
-                         double *final_res, const Deflation *def, cudaStream_t s) {
+                         double *final_res, Deflation *def, bool refresh, cudaStream_t s) {
   const int64_t n = G.n;
   VT *V = G.basis<VT>();
   std::vector<std::complex<double>> H((size_t)(m + 1) * m), cs(m), sn(m), gvec(m + 1), y(m);
   int64_t it = 0;
   double res = 0;
-  while (true) {
+  for (int cycle = 0;; cycle++) {
+    if (def && refresh && cycle > 0) refresh_deflation(PP, x, *def, s);
     // r = b - A x
     apply_A(PP, x, G.t, s);
     k_e0_minus<<<grid_for(n), NT, 0, s>>>(G.t, n);
@@ -642,7 +915,7 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
 // Returns iterations, fills x (device, length n).  rtol is relative to ||b|| = 1.
 // The basis precision follows quac_set_gmres_precision.
 int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, bool x_is_guess,
-                    double *final_res, const Deflation *def = nullptr) {
+                    double *final_res, Deflation *def = nullptr, bool refresh = false) {
   ensure_program(qs);
   const DeviceProgram &PP = *qs->impl->prog;
   const DevProg &P = PP.dev;
@@ -658,8 +931,8 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
     const double2 one = make_double2(1.0, 0.0);
     QCUDA(cudaMemcpyAsync(x, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
   }
-  return f32 ? gmres_run<float2>(PP, G, x, rtol, m, maxit, final_res, def, s)
-             : gmres_run<double2>(PP, G, x, rtol, m, maxit, final_res, def, s);
+  return f32 ? gmres_run<float2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s)
+             : gmres_run<double2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s);
 }
 
 }  // namespace quac
@@ -719,7 +992,8 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
   }
   double res = 0;
   const int m = options().gmres_restart;
-  int64_t its = gmres_solve(qs, x->data->d, 1e-11, m, maxit_guided, true, &res, use ? &F : nullptr);
+  int64_t its = gmres_solve(qs, x->data->d, 1e-11, m, maxit_guided, true, &res, use ? &F : nullptr,
+                            options().defl_refresh != 0);
   F.release();
   if (its < 0) return -1;
   if (res > 1e-11) {

@@ -114,6 +114,49 @@ def test_guided_steady_state_falls_back_to_plain_gmres(quac, oracle):
     B.qs.destroy()
 
 
+def test_deflation_refresh_finds_the_subspace_itself(quac, oracle):
+    """Started from e0 with an arbitrary U, the guided solve refreshes U
+    from the iterate at every restart (one Rayleigh-Ritz step); it meets
+    the residual bar in far fewer iterations than plain GMRES(100), and
+    with refresh off the same start gains little or nothing."""
+    ne, nc = 3, 4
+    xs, D = _oracle_steady(oracle, ne, nc, TC_POINT)
+    B = Sy.Builder(quac)
+    Sy.tavis_cummings(B, ne=ne, nc=nc, g=0.1, **TC_POINT)
+    quac.construct_matrix(B.qs)
+    cold = quac.create_qvec_sys(B.qs)
+    its_cold = quac.steady_state_sys(B.qs, cold)
+    e0 = np.zeros(D * D, complex)
+    e0[0] = 1.0
+    out = {}
+    for mode in (1, 0):
+        quac.set_deflation_refresh(mode)
+        try:
+            g = quac.create_qvec_sys(B.qs)
+            g.from_numpy(e0)
+            its, res = quac.steady_state_guided(B.qs, g, np.eye(D, 8, dtype=complex))
+        finally:
+            quac.set_deflation_refresh(1)
+        y = g.to_numpy()
+        assert res <= 1e-11
+        assert np.linalg.norm(y - xs) / np.linalg.norm(xs) < 1e-8
+        out[mode] = its
+        g.destroy()
+    print(f"cold {its_cold}, refresh on {out[1]}, refresh off {out[0]} iterations")
+    assert 3 * out[1] < its_cold
+    assert out[1] < out[0]
+    # kd up to 16 is accepted, 17 is not
+    g = quac.create_qvec_sys(B.qs)
+    g.from_numpy(e0)
+    its16, res16 = quac.steady_state_guided(B.qs, g, np.eye(D, 16, dtype=complex))
+    assert res16 <= 1e-11
+    with pytest.raises(quac.QuacError):
+        quac.steady_state_guided(B.qs, g, np.eye(D, 17, dtype=complex))
+    g.destroy()
+    cold.destroy()
+    B.qs.destroy()
+
+
 def _residual(oracle, ne, nc, p, x):
     import scipy.sparse as sp
     O = oracle.OSys()

@@ -196,6 +196,9 @@ void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t 
     CG = NT / TR;
     K = 8;
     while (K > 1 && (int64_t)CG * (K / 2) >= P.ncols) K /= 2;
+    // small systems: one column per thread, so the few CTAs there are
+    // split the work as finely as they can
+    if ((int64_t)P.D * P.ncols <= (int64_t)NT * 64) K = 1;
   }
   const int TC = CG * K;
   dim3 grid((P.D + TR - 1) / TR, (P.ncols + TC - 1) / TC);

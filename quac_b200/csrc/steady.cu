@@ -23,8 +23,16 @@ namespace quac {
 namespace {
 
 constexpr int NT = 256;
-constexpr int CHUNK = 1024;  // elements of w staged per block
+constexpr int CHUNK = 1024;  // largest chunk of w staged per block (multi-dot)
+constexpr int FUSE_NB = 32;  // small-n path (n <= FUSE_NB * 256): multi-dot partials per projection
+constexpr int CGS_EB = 32;   // small-n Gram-Schmidt: elements per block
+constexpr int CGS_KG = 8;    //   and k-groups per element (CGS_EB * CGS_KG threads)
 constexpr int GMRES_MAXM = 1024;  // largest restart length
+// Arnoldi steps are queued up to GMRES_LAG ahead of the host's Givens
+// updates; their Hessenberg columns come back through GMRES_RING slots.
+constexpr int GMRES_LAG = 2;
+constexpr int GMRES_RING = 4;
+static_assert(GMRES_RING > GMRES_LAG, "a slot is reused only after the host has read it");
 
 __device__ __forceinline__ double2 cmuls(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -62,16 +70,16 @@ __global__ void k_trace_add(const double2 *__restrict__ x, double2 *__restrict__
   }
 }
 
-// partial[k*nb + blk] = sum over this block's chunk of conj(V_k[i]) w[i].
-// The chunk of w is staged in shared memory; each warp then takes one basis
-// vector k = blockIdx.y * 8 + warp, so all projections run side by side
-// (grid nb x ceil(nk / 8)) instead of one after another.
+// partial[k*nb + blk] = sum over this block's chunk (chunk <= CHUNK
+// elements) of conj(V_k[i]) w[i].  The chunk of w is staged in shared
+// memory; each warp then takes one basis vector k = blockIdx.y * 8 + warp,
+// so all projections run side by side (grid nb x ceil(nk / 8)).
 template <typename VT>
 __global__ void k_multidot(const VT *__restrict__ V, const double2 *__restrict__ w, int64_t n,
-                           int nk, double2 *__restrict__ partial) {
+                           int nk, double2 *__restrict__ partial, int chunk) {
   __shared__ double2 ws[CHUNK];
-  const int64_t i0 = (int64_t)blockIdx.x * CHUNK;
-  const int len = (int)min((int64_t)CHUNK, n - i0);
+  const int64_t i0 = (int64_t)blockIdx.x * chunk;
+  const int len = (int)min((int64_t)chunk, n - i0);
   for (int i = threadIdx.x; i < len; i += NT) ws[i] = w[i0 + i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -185,12 +193,115 @@ __global__ void k_arnoldi_finish(double2 *__restrict__ h, const double2 *__restr
   }
 }
 
+// Small-n Gram-Schmidt pass (nb <= FUSE_NB multi-dot partials per
+// projection): every block sums the projections h_k = sum_b partial[k][b]
+// itself (fixed order; block 0 stores them in hout), then
+// w[i] -= sum_k h_k V_k[i] with CGS_KG k-groups per element, combined in a
+// fixed order.  NORM: npart[block] = sum of |w[i]|^2 over its elements.
+template <typename VT, bool NORM>
+__global__ void __launch_bounds__(CGS_EB * CGS_KG)
+k_cgs_small(const VT *__restrict__ V, const double2 *__restrict__ partial, int nb, int nk, int64_t n,
+            double2 *__restrict__ w, double2 *__restrict__ hout, double *__restrict__ npart) {
+  __shared__ double2 cs[GMRES_MAXM + 1];
+  __shared__ double2 red[CGS_KG][CGS_EB];
+  __shared__ double nred[CGS_EB / 32 > 0 ? CGS_EB / 32 : 1];
+  for (int k = threadIdx.x; k < nk; k += CGS_EB * CGS_KG) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int b = 0; b < nb; b++) {
+      const double2 v = partial[(size_t)k * nb + b];
+      acc.x += v.x; acc.y += v.y;
+    }
+    cs[k] = acc;
+    if (blockIdx.x == 0) hout[k] = acc;
+  }
+  __syncthreads();
+  const int e = threadIdx.x % CGS_EB, g = threadIdx.x / CGS_EB;
+  const int64_t i = (int64_t)blockIdx.x * CGS_EB + e;
+  double2 acc = make_double2(0.0, 0.0);
+  if (i < n) {
+#pragma unroll 4
+    for (int k = g; k < nk; k += CGS_KG) {
+      const double2 p = cmuls(cs[k], ldv(V + (size_t)k * n + i));
+      acc.x += p.x; acc.y += p.y;
+    }
+  }
+  red[g][e] = acc;
+  __syncthreads();
+  if (g == 0) {
+    double ss = 0.0;
+    if (i < n) {
+      double2 t = red[0][e];
+      for (int q = 1; q < CGS_KG; q++) { t.x += red[q][e].x; t.y += red[q][e].y; }
+      double2 wi = w[i];
+      wi.x -= t.x;
+      wi.y -= t.y;
+      w[i] = wi;
+      ss = wi.x * wi.x + wi.y * wi.y;
+    }
+    if (NORM) {
+      for (int o = 16; o > 0; o >>= 1) ss += __shfl_down_sync(0xffffffffu, ss, o);
+      if ((e & 31) == 0) nred[e >> 5] = ss;
+    }
+  }
+  if (NORM) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int q = 0; q < (CGS_EB + 31) / 32; q++) t += nred[q];
+      npart[blockIdx.x] = t;
+    }
+  }
+}
+
+// Small-n end of an Arnoldi step: every block sums the nparts partial norms
+// (fixed order), block 0 completes the Hessenberg column (hj[k] += h2[k],
+// hj[nk] = ||w||), and all blocks write vnext = w / ||w|| (0 if ||w|| = 0).
+template <typename VT>
+__global__ void k_finish_scale(double2 *__restrict__ hj, const double2 *__restrict__ h2, int nk,
+                               const double *__restrict__ npart, int nparts, const double2 *__restrict__ w,
+                               VT *__restrict__ vnext, int64_t n) {
+  __shared__ double nv;
+  if (threadIdx.x < 32) {
+    double t = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += 32) t += npart[b];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) nv = sqrt(t);
+  }
+  __syncthreads();
+  const double norm = nv;
+  if (blockIdx.x == 0) {
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+      hj[k].x += h2[k].x;
+      hj[k].y += h2[k].y;
+    }
+    if (threadIdx.x == 0) hj[nk] = make_double2(norm, 0.0);
+  }
+  const double sc = norm > 0.0 ? 1.0 / norm : 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = w[i];
+    stv(vnext + i, make_double2(v.x * sc, v.y * sc));
+  }
+}
+
 // out = in * s (s real); also used to copy and convert (s = 1)
 template <typename TI, typename TO>
 __global__ void k_scale(const TI *__restrict__ in, TO *__restrict__ out, int64_t n, double s) {
   for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
     const double2 v = ldv(in + i);
     stv(out + i, make_double2(v.x * s, v.y * s));
+  }
+}
+
+// out = w / hn->x (0 if hn->x is 0): the next basis vector, scaled by the
+// norm the Arnoldi step left on the device
+template <typename VT>
+__global__ void k_scale_by_norm(const double2 *__restrict__ w, VT *__restrict__ out, int64_t n,
+                                const double2 *__restrict__ hn) {
+  const double nv = hn->x;
+  const double sc = nv > 0.0 ? 1.0 / nv : 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    const double2 v = w[i];
+    stv(out + i, make_double2(v.x * sc, v.y * sc));
   }
 }
 
@@ -328,6 +439,57 @@ __global__ void k_defl_expand(const double2 *__restrict__ in, double2 *__restric
   }
 }
 
+// Small-n deflation with W and AW = A W stored explicitly (K2 vectors of n
+// each): w <- w - AW (Ei z), z_p = sum_b partial[p][b] = (W^H w)_p from the
+// multi-dot.  Every block sums z and forms c = Ei z itself (fixed order);
+// each element's sum over q is split over CGS_KG groups combined in a
+// fixed order.
+__global__ void __launch_bounds__(CGS_EB * CGS_KG)
+k_defl_apply_small(const double2 *__restrict__ AW, const double2 *__restrict__ Ei,
+                   const double2 *__restrict__ partial, int nb, int K2, int64_t n, double2 *__restrict__ w) {
+  __shared__ double2 z[KDMAX * KDMAX];
+  __shared__ double2 c[KDMAX * KDMAX];
+  __shared__ double2 red[CGS_KG][CGS_EB];
+  for (int p = threadIdx.x; p < K2; p += CGS_EB * CGS_KG) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int b = 0; b < nb; b++) {
+      const double2 v = partial[(size_t)p * nb + b];
+      acc.x += v.x; acc.y += v.y;
+    }
+    z[p] = acc;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < K2; q += CGS_EB * CGS_KG) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int p = 0; p < K2; p++) {
+      const double2 t = cmuls(Ei[(size_t)q * K2 + p], z[p]);
+      acc.x += t.x; acc.y += t.y;
+    }
+    c[q] = acc;
+  }
+  __syncthreads();
+  const int e = threadIdx.x % CGS_EB, g = threadIdx.x / CGS_EB;
+  const int64_t i = (int64_t)blockIdx.x * CGS_EB + e;
+  double2 acc = make_double2(0.0, 0.0);
+  if (i < n) {
+#pragma unroll 4
+    for (int q = g; q < K2; q += CGS_KG) {
+      const double2 t = cmuls(c[q], AW[(size_t)q * n + i]);
+      acc.x += t.x; acc.y += t.y;
+    }
+  }
+  red[g][e] = acc;
+  __syncthreads();
+  if (g == 0 && i < n) {
+    double2 t = red[0][e];
+    for (int q = 1; q < CGS_KG; q++) { t.x += red[q][e].x; t.y += red[q][e].y; }
+    double2 wi = w[i];
+    wi.x -= t.x;
+    wi.y -= t.y;
+    w[i] = wi;
+  }
+}
+
 // Y += (X Z) / 2 for X (D x D) and Z (D x k, k <= KDMAX), both column-major:
 // thread = row r, block column = a segment of XSEG columns of X, segments
 // summed with atomics (Y zeroed by the caller).
@@ -419,44 +581,60 @@ int grid_for(int64_t n) {
 // basis V holds complex128 or, in the FP32-inner solver, complex64 vectors;
 // the residual t and the work vector w are always complex128.
 struct Gmres {
-  int m = 0, f32 = 0;
+  int m = 0, f32 = 0, mcap = 0;  // restart length and basis precision of this solve; capacity
   int64_t n = 0;
-  void *V = nullptr;           // (m+1) x n basis vectors
+  void *V = nullptr;           // (mcap+1) x n basis vectors (sized for complex128)
   double2 *t = nullptr;        // residual / conversion buffer
   double2 *w = nullptr;
   double2 *partial = nullptr;  // (m+1) x nb
-  double2 *h = nullptr;        // m+2: projections, then the norm
+  double2 *h = nullptr;        // m+2: the least-squares solution y of a cycle
+  double2 *hd = nullptr;       // RING slots of m+2: Hessenberg columns (projections, then the norm)
   double2 *h2 = nullptr;       // second-pass projections
   double *npart = nullptr;     // per-block partial norms
-  double2 *hh = nullptr;       // pinned host copy of h
-  int nb = 0;
+  double2 *hh = nullptr;       // pinned host copy of the RING slots
+  cudaEvent_t ev[GMRES_RING] = {};
+  int nb = 0, chunk = CHUNK;  // multi-dot partials per projection, elements per partial
+  bool small() const { return chunk == 256; }
   template <typename VT> VT *basis() const { return static_cast<VT *>(V); }
+  // Buffers are kept across solves and reallocated only for a new n or a
+  // longer restart, so solves that alternate settings reuse them.
   void ensure(int64_t n_, int m_, int f32_) {
-    if (n_ == n && m_ == m && f32_ == f32) return;
+    f32 = f32_;
+    if (n_ == n && m_ <= mcap) {
+      m = m_;
+      return;
+    }
     release();
     n = n_;
-    m = m_;
+    m = mcap = m_;
     f32 = f32_;
-    nb = (int)((n + CHUNK - 1) / CHUNK);
-    QCUDA(cudaMalloc(&V, (size_t)(m + 1) * n * (f32 ? sizeof(float2) : sizeof(double2))));
+    chunk = n <= (int64_t)FUSE_NB * 256 ? 256 : CHUNK;
+    nb = (int)((n + chunk - 1) / chunk);
+    QCUDA(cudaMalloc(&V, (size_t)(m + 1) * n * sizeof(double2)));
     QCUDA(cudaMalloc(&t, (size_t)n * sizeof(double2)));
     QCUDA(cudaMalloc(&w, (size_t)n * sizeof(double2)));
     QCUDA(cudaMalloc(&partial, (size_t)(m + 1) * nb * sizeof(double2)));
     QCUDA(cudaMalloc(&h, (size_t)(m + 2) * sizeof(double2)));
+    QCUDA(cudaMalloc(&hd, (size_t)GMRES_RING * (m + 2) * sizeof(double2)));
     QCUDA(cudaMalloc(&h2, (size_t)(m + 1) * sizeof(double2)));
-    QCUDA(cudaMalloc(&npart, (size_t)grid_for(n) * sizeof(double)));
-    QCUDA(cudaMallocHost(&hh, (size_t)(m + 2) * sizeof(double2)));
+    QCUDA(cudaMalloc(&npart, (size_t)std::max<int64_t>(grid_for(n), (n + CGS_EB - 1) / CGS_EB) * sizeof(double)));
+    QCUDA(cudaMallocHost(&hh, (size_t)GMRES_RING * (m + 2) * sizeof(double2)));
+    for (cudaEvent_t &e : ev) QCUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   void release() {
     if (V) {
-      cudaFree(V); cudaFree(t); cudaFree(w); cudaFree(partial); cudaFree(h); cudaFree(h2); cudaFree(npart);
+      cudaFree(V); cudaFree(t); cudaFree(w); cudaFree(partial); cudaFree(h); cudaFree(hd); cudaFree(h2);
+      cudaFree(npart);
       cudaFreeHost(hh);
+      for (cudaEvent_t &e : ev)
+        if (e) cudaEventDestroy(e);
     }
+    for (cudaEvent_t &e : ev) e = nullptr;
     V = nullptr;
-    t = w = partial = h = h2 = hh = nullptr;
+    t = w = partial = h = hd = h2 = hh = nullptr;
     npart = nullptr;
     n = 0;
-    m = 0;
+    m = mcap = 0;
   }
 };
 
@@ -466,6 +644,7 @@ struct GmresSlot {
   Gmres g;
   std::mutex mu;
 };
+
 
 static GmresSlot &gmres_slot() {
   static std::mutex mu;
@@ -507,11 +686,16 @@ struct Deflation {
   double2 *U = nullptr, *Ei = nullptr, *partial = nullptr, *coef = nullptr, *t1 = nullptr, *t2 = nullptr;
   double2 *Y = nullptr, *Z = nullptr;    // D x KDMAX each (subspace refresh)
   double2 *Id = nullptr, *Ecol = nullptr;  // kd^2 x kd^2 each (assembly of E)
+  // small n: W and AW stored (kd^2 x n each) and the multi-dot partials of W^H w
+  double2 *W = nullptr, *AW = nullptr, *pw = nullptr;
+  int nbw = 0;
+  bool stored() const { return W != nullptr; }
   std::vector<std::complex<double>> Uh;  // host copy of U, column-major D x kd
+  int cap = 0;                           // kd the buffers were sized for
   void release() {
-    for (double2 *p : {U, Ei, partial, coef, t1, t2, Y, Z, Id, Ecol})
+    for (double2 *p : {U, Ei, partial, coef, t1, t2, Y, Z, Id, Ecol, W, AW, pw})
       if (p) cudaFree(p);
-    U = Ei = partial = coef = t1 = t2 = Y = Z = Id = Ecol = nullptr;
+    U = Ei = partial = coef = t1 = t2 = Y = Z = Id = Ecol = W = AW = pw = nullptr;
   }
 };
 
@@ -530,8 +714,16 @@ static void apply_Q(const Deflation &F, const double2 *in, double2 *out, cudaStr
   count_launch();
 }
 
-// w <- P w = w - A Q w   (uses t1, t2)
+// w <- P w = w - A Q w   (uses t1, t2; small n: W^H w and AW from storage, two launches)
 static void apply_P(const DeviceProgram &PP, const Deflation &F, double2 *w, int64_t n, cudaStream_t s) {
+  if (F.stored()) {
+    const int K2 = F.kd * F.kd;
+    k_multidot<double2><<<dim3(F.nbw, (K2 + NT / 32 - 1) / (NT / 32)), NT, 0, s>>>(F.W, w, n, K2, F.pw, 256);
+    k_defl_apply_small<<<(int)((n + CGS_EB - 1) / CGS_EB), CGS_EB * CGS_KG, 0, s>>>(F.AW, F.Ei, F.pw, F.nbw,
+                                                                                     K2, n, w);
+    count_launch(2);
+    return;
+  }
   apply_Q(F, w, F.t1, s);
   apply_A(PP, F.t1, F.t2, s);
   k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(w, F.t2, n, -1.0);
@@ -612,11 +804,18 @@ static void herm_eig(std::vector<cplx> &A, int n, std::vector<double> &w, std::v
   for (int i = 0; i < n; i++) w[i] = A[(size_t)i * n + i].real();
 }
 
+// Sizes the buffers for rank kd; a workspace already sized for this D and
+// at least this rank is reused as it is.
 static bool alloc_deflation(const DeviceProgram &PP, int kd, Deflation &F) {
   const int D = PP.dev.D;
   const int64_t n = (int64_t)D * D;
+  if (F.U && F.D == D && F.cap >= kd) {
+    F.kd = kd;
+    return true;
+  }
+  F.release();
   F.D = D;
-  F.kd = kd;
+  F.kd = F.cap = kd;
   F.nbx = (D + DR - 1) / DR;
   F.nby = (D + DC - 1) / DC;
   const int K2 = kd * kd;
@@ -630,6 +829,12 @@ static bool alloc_deflation(const DeviceProgram &PP, int kd, Deflation &F) {
   QCUDA(cudaMalloc(&F.Z, (size_t)D * KDMAX * sizeof(double2)));
   QCUDA(cudaMalloc(&F.Id, (size_t)K2 * K2 * sizeof(double2)));
   QCUDA(cudaMalloc(&F.Ecol, (size_t)K2 * K2 * sizeof(double2)));
+  if (n <= (int64_t)FUSE_NB * 256) {
+    F.nbw = (int)((n + 255) / 256);
+    QCUDA(cudaMalloc(&F.W, (size_t)K2 * n * sizeof(double2)));
+    QCUDA(cudaMalloc(&F.AW, (size_t)K2 * n * sizeof(double2)));
+    QCUDA(cudaMalloc(&F.pw, (size_t)K2 * F.nbw * sizeof(double2)));
+  }
   return !has_error();
 }
 
@@ -642,11 +847,14 @@ static bool assemble_E(const DeviceProgram &PP, Deflation &F, cudaStream_t s) {
   std::vector<double2> hId((size_t)K2 * K2, make_double2(0.0, 0.0)), hE((size_t)K2 * K2);
   for (int q = 0; q < K2; q++) hId[(size_t)q * K2 + q] = make_double2(1.0, 0.0);
   QCUDA(cudaMemcpyAsync(F.Id, hId.data(), hId.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
-  for (int q = 0; q < K2; q++) {
-    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, F.t1, F.U, F.Id + (size_t)q * K2, F.D, kd);
+  const int64_t n = (int64_t)F.D * F.D;
+  for (int q = 0; q < K2; q++) {  // small n: W_q and A W_q are kept
+    double2 *wq = F.stored() ? F.W + (size_t)q * n : F.t1;
+    double2 *awq = F.stored() ? F.AW + (size_t)q * n : F.t2;
+    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, wq, F.U, F.Id + (size_t)q * K2, F.D, kd);
     count_launch();
-    apply_A(PP, F.t1, F.t2, s);
-    defl_project(F, F.t2, nullptr, F.Ecol + (size_t)q * K2, 0, s);
+    apply_A(PP, wq, awq, s);
+    defl_project(F, awq, nullptr, F.Ecol + (size_t)q * K2, 0, s);
   }
   QCUDA(cudaMemcpyAsync(hE.data(), F.Ecol, hE.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));
@@ -793,9 +1001,10 @@ static bool refresh_deflation(const DeviceProgram &PP, const double2 *x, Deflati
   }
   F.Uh = Un;
   upload_U(F, s);
-  if (!assemble_E(PP, F, s)) {
+  if (!assemble_E(PP, F, s)) {  // keep the previous subspace (and its stored W, AW, E^-1)
     F.Uh = U;
     upload_U(F, s);
+    assemble_E(PP, F, s);
     return false;
   }
   return !has_error();
@@ -814,6 +1023,7 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
   int64_t it = 0;
   double res = 0;
   for (int cycle = 0;; cycle++) {
+    if (has_error()) break;
     if (def && refresh && cycle > 0) refresh_deflation(PP, x, *def, s);
     // r = b - A x
     apply_A(PP, x, G.t, s);
@@ -835,8 +1045,11 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
     count_launch();
     std::fill(gvec.begin(), gvec.end(), 0.0);
     gvec[0] = beta;
-    int j = 0;
-    for (; j < m && it < maxit; j++, it++) {
+    // Arnoldi steps run ahead of the host by up to GMRES_LAG: step j needs
+    // only V_j, which step j-1 scaled on the device, so the host queues
+    // the next steps before it reads column j back and applies the Givens
+    // rotations.  Steps queued past convergence are discarded.
+    auto launch_step = [&](int j) {
       const VT *vj = V + (size_t)j * n;
       if constexpr (std::is_same<VT, double2>::value) {
         apply_A(PP, reinterpret_cast<const double2 *>(vj), G.w, s);
@@ -846,26 +1059,42 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
         apply_A(PP, G.t, G.w, s);
       }
       if (def) apply_P(PP, *def, G.w, n, s);  // Arnoldi on P A
-      // CGS2 on the device; one copy of the Hessenberg column (projections
-      // of both passes summed, then ||w||) comes back per step
+      // CGS2 on the device; the Hessenberg column (projections of both
+      // passes summed, then ||w||) goes to ring slot j % GMRES_RING
+      double2 *hj = G.hd + (size_t)(j % GMRES_RING) * (m + 2);
       const dim3 gd(G.nb, (j + 1 + NT / 32 - 1) / (NT / 32));
-      k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial);
-      k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, G.h, 0);
-      k_multiaxpy<<<grid_for(n), NT, 0, s>>>(V, G.h, n, j + 1, G.w, -1.0);
-      k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial);
-      k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, G.h2, 0);
-      k_multiaxpy_norm<<<grid_for(n), NT, 0, s>>>(V, G.h2, n, j + 1, G.w, G.npart);
-      k_arnoldi_finish<<<1, NT, 0, s>>>(G.h, G.h2, j + 1, G.npart, grid_for(n));
-      count_launch(7);
-      QCUDA(cudaMemcpyAsync(G.hh, G.h, (j + 2) * sizeof(double2), cudaMemcpyDeviceToHost, s));
-      QCUDA(cudaStreamSynchronize(s));
-      const double hn = G.hh[j + 1].x;
-      for (int k = 0; k <= j; k++) H[(size_t)k * m + j] = std::complex<double>(G.hh[k].x, G.hh[k].y);
-      H[(size_t)(j + 1) * m + j] = hn;
-      if (hn > 0) {
-        k_scale<<<grid_for(n), NT, 0, s>>>(G.w, V + (size_t)(j + 1) * n, n, 1.0 / hn);
-        count_launch();
+      if (G.small()) {  // few partials: 5 launches, reductions inside the CGS passes
+        const int nbl = (int)((n + CGS_EB - 1) / CGS_EB);
+        k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial, G.chunk);
+        k_cgs_small<VT, false><<<nbl, CGS_EB * CGS_KG, 0, s>>>(V, G.partial, G.nb, j + 1, n, G.w, hj, nullptr);
+        k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial, G.chunk);
+        k_cgs_small<VT, true><<<nbl, CGS_EB * CGS_KG, 0, s>>>(V, G.partial, G.nb, j + 1, n, G.w, G.h2, G.npart);
+        k_finish_scale<<<grid_for(n), NT, 0, s>>>(hj, G.h2, j + 1, G.npart, nbl, G.w, V + (size_t)(j + 1) * n, n);
+        count_launch(5);
+      } else {
+        k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial, G.chunk);
+        k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, hj, 0);
+        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(V, hj, n, j + 1, G.w, -1.0);
+        k_multidot<<<gd, NT, 0, s>>>(V, G.w, n, j + 1, G.partial, G.chunk);
+        k_reduce_rows<<<j + 1, NT, 0, s>>>(G.partial, G.nb, G.h2, 0);
+        k_multiaxpy_norm<<<grid_for(n), NT, 0, s>>>(V, G.h2, n, j + 1, G.w, G.npart);
+        k_arnoldi_finish<<<1, NT, 0, s>>>(hj, G.h2, j + 1, G.npart, grid_for(n));
+        k_scale_by_norm<<<grid_for(n), NT, 0, s>>>(G.w, V + (size_t)(j + 1) * n, n, hj + j + 1);
+        count_launch(8);
       }
+      QCUDA(cudaMemcpyAsync(G.hh + (size_t)(j % GMRES_RING) * (m + 2), hj, (j + 2) * sizeof(double2),
+                            cudaMemcpyDeviceToHost, s));
+      QCUDA(cudaEventRecord(G.ev[j % GMRES_RING], s));
+    };
+    int jl = 0, j = 0;  // steps launched, steps processed
+    while (true) {
+      while (jl < m && jl - j <= GMRES_LAG && it + (jl - j) < maxit) launch_step(jl++);
+      if (j >= jl || has_error()) break;
+      QCUDA(cudaEventSynchronize(G.ev[j % GMRES_RING]));
+      const double2 *hc = G.hh + (size_t)(j % GMRES_RING) * (m + 2);
+      const double hn = hc[j + 1].x;
+      for (int k = 0; k <= j; k++) H[(size_t)k * m + j] = std::complex<double>(hc[k].x, hc[k].y);
+      H[(size_t)(j + 1) * m + j] = hn;
       for (int k = 0; k < j; k++) {
         auto a = H[(size_t)k * m + j], b = H[(size_t)(k + 1) * m + j];
         H[(size_t)k * m + j] = std::conj(cs[k]) * a + std::conj(sn[k]) * b;
@@ -879,7 +1108,9 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
       H[(size_t)(j + 1) * m + j] = 0;
       gvec[j + 1] = -sn[j] * gvec[j];
       gvec[j] = std::conj(cs[j]) * gvec[j];
-      if (std::abs(gvec[j + 1]) <= rtol || hn == 0) { j++; it++; break; }
+      j++;
+      it++;
+      if (std::abs(gvec[j]) <= rtol || hn == 0) break;
     }
     // solve the triangular system and update x += V y
     for (int k = j - 1; k >= 0; k--) {
@@ -950,6 +1181,19 @@ extern "C" PetscInt steady_state_sys(qsystem qs, qvec x) {
   return has_error() ? -1 : its;
 }
 
+// Deflation workspace of one device, kept across guided solves (used under
+// the lock of the device's GMRES workspace).
+static Deflation &deflation_slot() {
+  static std::mutex mu;
+  static std::map<int, std::unique_ptr<Deflation>> slots;
+  int dev = 0;
+  QCUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  std::unique_ptr<Deflation> &p = slots[dev];
+  if (!p) p.reset(new Deflation());
+  return *p;
+}
+
 // Steady state from a proposed initial state (x on entry) and a proposed
 // dominant subspace U (D x kd, orthonormal columns, column-major host array;
 // kd = 0: no deflation).  Deflated GMRES runs for at most maxit_guided
@@ -966,10 +1210,10 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
   const DeviceProgram &PP = *qs->impl->prog;
   cudaStream_t s = stream_of(qs);
   std::lock_guard<std::mutex> lk(gmres_slot().mu);
-  Deflation F;
+  Deflation &F = deflation_slot();
   const bool use = kd > 0;
   if (use && !build_deflation(PP, reinterpret_cast<const std::complex<double> *>(U_host), (int)kd, F, s)) {
-    F.release();
+    if (!has_error()) fail(0, "ERROR! W^H A W is singular for the proposed deflation space\n");
     return -1;
   }
   // start from whichever of the proposal and e0 has the smaller residual
@@ -994,7 +1238,6 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
   const int m = options().gmres_restart;
   int64_t its = gmres_solve(qs, x->data->d, 1e-11, m, maxit_guided, true, &res, use ? &F : nullptr,
                             options().defl_refresh != 0);
-  F.release();
   if (its < 0) return -1;
   if (res > 1e-11) {
     const int64_t more = gmres_solve(qs, x->data->d, 1e-11, m, 200000, true, &res);

@@ -67,13 +67,24 @@ def main():
     loss = net.train(a.steps, lr=a.lr, seed=3)
     t_train = time.perf_counter() - t
 
+    # untimed warm-up of every arm on a training point: the first solve of a
+    # solver setting in a process loads its kernels and sizes its buffers
+    plain_settings()
+    WS.solve_cold(q, train[0], a.ne, a.nc)
+    learned_settings()
+    e0 = np.zeros(D * D, complex)
+    e0[0] = 1.0
+    for x0, U in ((e0, np.eye(D, a.kd, dtype=complex)),
+                  WS.proposal_from_factors(net.predict(WS.normalize(train[0])[None, :])[0], a.kd)):
+        B, v, _, _, _ = WS.solve_guided(q, train[0], a.ne, a.nc, x0, U)
+        v.destroy()
+        B.qs.destroy()
+
     rows = []
     for th in held:
         plain_settings()
         xc, its_c, dt_c = WS.solve_cold(q, th, a.ne, a.nc)
         learned_settings()
-        e0 = np.zeros(D * D, complex)
-        e0[0] = 1.0
         B, v, its_m, _, dt_m = WS.solve_guided(q, th, a.ne, a.nc, e0, np.eye(D, a.kd, dtype=complex))
         xm = v.to_numpy()
         v.destroy()

@@ -366,6 +366,21 @@ def circuit_summary(q, nq=10, layers=40):
     return out
 
 
+def steady_summary(q):
+    """Learned warm start for steady states, at the scale that fits the
+    bench: driven Tavis-Cummings with 3 emitters and 4 cavity levels
+    (D = 32), a 2-D sweep of (Omega, Delta), 48 solver-generated training
+    states, 12 held-out points.  Solves/s of plain complex128 GMRES(100)
+    from e0 against the learned start (FP32-inner / FP64-refined GMRES(300),
+    deflation refreshed every restart), and the same solver without the
+    network."""
+    from quac_b200 import steady_probe
+    out = steady_probe.run_sweep(q, steady_probe.defaults(sweep2d=True, restart=300))
+    return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "solver", "cold", "method",
+                                "learned", "learned_vs_cold", "learned_vs_method", "method_vs_cold",
+                                "pop_err_max", "residual_max")}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import quac_b200 as q
@@ -463,6 +478,7 @@ def run_ours(args, rank, world, local_rank):
         out["ensemble"] = ensemble_summary(q)
         out["jc"] = jc_summary(q)
         out["circuit"] = circuit_summary(q)
+        out["steady_state"] = steady_summary(q)
     q.set_ts_options(rk_type="3bs", adapt_type="basic")
     rho.destroy()
     qs.destroy()
@@ -477,7 +493,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true",
-                    help="skip the sections beside the headline (complex64, ensemble, JC, circuit)")
+                    help="skip the sections beside the headline (complex64, ensemble, JC, circuit, steady state)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

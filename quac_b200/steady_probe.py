@@ -27,6 +27,15 @@ import numpy as np
 from . import warmstart as WS
 
 
+def defaults(**kw):
+    """The command-line defaults as an attribute object, overridden by kw."""
+    a = argparse.Namespace(ne=3, nc=4, train=48, held=12, sweep2d=False, steps=8000, lr=2e-3, fp32=1, kd=8,
+                           seed=5, restart=100, refresh=1)
+    for k, v in kw.items():
+        setattr(a, k, v)
+    return a
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ne", type=int, default=3)
@@ -44,7 +53,12 @@ def main():
     a = ap.parse_args()
     import quac_b200 as q
     q.QuaC_initialize()
+    print(json.dumps(run_sweep(q, a)))
 
+
+def run_sweep(q, a):
+    """The measurement described in the module docstring; `a` carries the
+    command-line settings as attributes."""
     D = 2 ** a.ne * a.nc
     fixed = {2: 0.1, 3: 5e-3} if a.sweep2d else None
     thetas = WS.sweep_params(a.train + a.held, seed=a.seed, fixed=fixed)
@@ -122,7 +136,7 @@ def main():
         "residual_max": float(r[:, 7].max()),
     }
     net.destroy()
-    print(json.dumps(out))
+    return out
 
 
 if __name__ == "__main__":

@@ -3,8 +3,10 @@
 Workload: the 12-qubit open transverse-field Ising chain (Hilbert D = 4096,
 rho = 16.8M complex128 = 268 MB, 47 terms: 11 ZZ + 12 X Hamiltonian terms,
 12 decay + 12 dephasing Lindblad terms; J ~ U[0.5,1.5], h ~ N(0, 0.2^2)
-from a seeded generator).  One bench step is one integration segment of 10
-fixed RK4 steps (dt = 0.01), i.e. 40 fused L.rho stage launches.
+from a seeded generator).  One bench step is one integration segment of 25
+fixed RK4 steps (dt = 0.01), i.e. 100 fused L.rho stage launches (one
+time_step_sys call, whose host round trips are thus amortised over 100
+applications).
 
 metric: L.rho GB/s = applications x 32*D^2 algorithmic bytes (read rho,
 write L rho, 16 B each per element) / time.  `value` has rho resident in
@@ -33,7 +35,7 @@ sys.path.insert(0, ROOT)
 METRIC = "L·ρ GB/s; ensemble & steady-state solves/s vs plain FP64 GPU at ≤1e-8 error"
 NQ = 12
 DT = 0.01
-RK_STEPS = 10
+RK_STEPS = 25
 STAGES = 4 * RK_STEPS
 
 
@@ -146,7 +148,7 @@ def cpu_baseline(seconds=12.0, rows_frac=64):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    # each step: one RK4 segment's worth (40 applications) of CSR SpMV on the sample rows
+    # each step: one RK4 segment's worth (STAGES applications) of CSR SpMV on the sample rows
     from oracle import oracle as O
     import ctypes
     S = O.OSys()
@@ -409,6 +411,25 @@ def run_ours(args, rank, world, local_rank):
         q.time_step_sys(qs, rho, t, t + RK_STEPS * DT, DT, 10 ** 9)
 
     t = 0.0
+    # Settle: on freshly acquired boxes this kernel has run 3-5x slower for
+    # stretches of seconds at normal clocks and normal copy bandwidth (cause
+    # outside this process).  Untimed segments run until three in a row agree
+    # within 5 % and are within 1.3x of the fastest seen, for at most 60 s;
+    # the W warm-up steps and the timed K steps follow.
+    settle_t0, times = time.perf_counter(), []
+    while time.perf_counter() - settle_t0 < 60.0:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        segment(t)
+        e1.record(stream)
+        e1.synchronize()
+        t += RK_STEPS * DT
+        times.append(e0.elapsed_time(e1))
+        last = times[-3:]
+        if len(last) == 3 and max(last) <= 1.05 * min(last) and max(last) <= 1.3 * min(times):
+            break
+    settle = {"seconds": time.perf_counter() - settle_t0, "segments": len(times),
+              "first_ms": times[0], "last_ms": times[-1]}
     for _ in range(args.warmup):
         segment(t)
         t += RK_STEPS * DT
@@ -468,6 +489,7 @@ def run_ours(args, rank, world, local_rank):
                      "per": "one L.rho application (32*D^2 algorithmic bytes)"},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "settle": settle,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()

@@ -267,6 +267,7 @@ void destroy_system(qsystem *qsys) {
   if (!q) return;
   clear_mat_terms_sys(q);
   q->impl->ws.release();
+  if (q->impl->host_vec) vec_free(q->impl->host_vec);
   if (q->impl->ws.dsum) cudaFree(q->impl->ws.dsum);
   if (q->impl->ws.hsum) cudaFreeHost(q->impl->ws.hsum);
   if (q->impl->stream) cudaStreamDestroy(q->impl->stream);

@@ -115,8 +115,7 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
   cudaStream_t s = stream_of(qs);
   Workspace &W = qs->impl->ws;
   W.ensure(n, dp5 ? 8 : 4);
-  vec_sync_to_device(v);
-  QCUDA(cudaDeviceSynchronize());
+  vec_sync_to_device(v);  // blocking copy of pending host values; everything else is ordered on s
 
   std::vector<Event> events = x ? collect_events(qs, t0, tmax) : std::vector<Event>();
   // Hermitian mode: L preserves Hermiticity (checked on the compiled
@@ -257,8 +256,10 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
       qs->ts_monitor(&ts, steps, t, v, qs->ts_ctx);
     }
   }
-  QCUDA(cudaStreamSynchronize(s));
-  check_program_error(*qs->impl->prog, s);
+  // one wait at the end: the error-flag read-back is queued behind the last
+  // stage (check_program_error synchronises), or a plain stream sync
+  if (qs->impl->prog->errflag) check_program_error(*qs->impl->prog, s);
+  else QCUDA(cudaStreamSynchronize(s));
   qs->current_time = t;
   if (std::fabs(t - tmax) > 1e-8 && !has_error()) printf("ERROR! Did not reach final time! Reason: %d\n", -1);
   return has_error() ? 1 : 0;
@@ -322,14 +323,19 @@ int quac_time_step_host(qsystem qs, PetscScalar *x_host, PetscReal t0, PetscReal
                         PetscReal dt, PetscInt steps_max) {
   if (qs->mat_allocated != 1) { fail(0, "ERROR! call construct_matrix first\n"); return 1; }
   const int64_t n = qs->dim;
-  Vec v = vec_new(n);
+  Vec &v = qs->impl->host_vec;  // device copy kept for the next call
+  if (v && vec_len(v) != n) {
+    vec_free(v);
+    v = nullptr;
+  }
+  if (!v) v = vec_new(n);
+  if (has_error()) return 1;
   cudaStream_t s = stream_of(qs);
   QCUDA(cudaMemcpyAsync(v->d, x_host, n * sizeof(double2), cudaMemcpyHostToDevice, s));
   QCUDA(cudaStreamSynchronize(s));
   int rc = integrate(qs, nullptr, v, t0, tmax, dt, steps_max);
   QCUDA(cudaMemcpyAsync(x_host, v->d, n * sizeof(double2), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));
-  vec_free(v);
   return rc;
 }
 

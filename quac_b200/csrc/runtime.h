@@ -65,6 +65,7 @@ struct qsystem_impl {
   cudaStream_t user_stream = nullptr;  // set by quac_set_stream (not owned)
   quac::Workspace ws;
   std::vector<op_handle> owned_ops;  // every operator struct created for this system
+  Vec host_vec = nullptr;            // device state of quac_time_step_host, kept between calls
 };
 
 namespace quac {

@@ -159,10 +159,15 @@ struct DeviceProgram {
 DeviceProgram *compile_terms(qsystem qs, int mode);
 
 // Kernel launchers (lrho.cu, lrho_qubit.cu)
-void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t s);
+// nbatch > 1: y_z = L x_z for nbatch vectors stored one after another
+// (e.kout only; no stage updates or norms)
+void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t s, int nbatch = 1);
 void launch_lrho_qubit(const DeviceProgram &P, const double2 *x, const Epi &e, cudaStream_t s);
 // Dispatch: the qubit kernel when the program has one, else the generic one.
 void launch_lrho_any(const DeviceProgram &P, const double2 *x, const Epi &e, cudaStream_t s);
+// y_z = L x_z, z < nbatch, in one launch (vectors stored one after
+// another); false (nothing launched) where the program runs a qubit kernel
+bool launch_lrho_batch(const DeviceProgram &P, const double2 *x, double2 *y, int nbatch, cudaStream_t s);
 bool compile_qubit(qsystem qs, const HostProg &hp, DeviceProgram *P);
 bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out);
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,

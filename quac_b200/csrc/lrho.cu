@@ -33,12 +33,19 @@ __device__ __forceinline__ void cfma(double2 &acc, double2 a, double2 b) {
 }
 __device__ __forceinline__ double cabs2(double2 a) { return sqrt(a.x * a.x + a.y * a.y); }
 
+// Batched form (gridDim.z > 1, epilogue writing kout only): slice z reads
+// X + z*D*ncols and writes kout + z*D*ncols.
 template <int K>
 __global__ void __launch_bounds__(NT) k_lrho(const DevProg P, const double2 *__restrict__ X,
-                                             const Epi E, const int TR, const int CG) {
+                                             Epi E, const int TR, const int CG) {
   extern __shared__ double2 tile[];
   __shared__ double red[NT / 32];
   const int D = P.D, NC = P.ncols;
+  if (blockIdx.z) {
+    const size_t zoff = (size_t)blockIdx.z * D * NC;
+    X += zoff;
+    E.kout += zoff;
+  }
   const int TC = CG * K;
   const int R0 = blockIdx.x * TR;
   const int C0 = blockIdx.y * TC;
@@ -185,7 +192,7 @@ void zero_epi(Epi &e) {
   e.yn_upd = -1;
 }
 
-void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t s) {
+void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t s, int nbatch) {
   int TR, CG, K;
   if (P.ncols == 1) {
     TR = P.D < NT ? P.D : NT;
@@ -201,7 +208,7 @@ void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t 
     if ((int64_t)P.D * P.ncols <= (int64_t)NT * 64) K = 1;
   }
   const int TC = CG * K;
-  dim3 grid((P.D + TR - 1) / TR, (P.ncols + TC - 1) / TC);
+  dim3 grid((P.D + TR - 1) / TR, (P.ncols + TC - 1) / TC, nbatch);
   const size_t smem = (size_t)TR * TC * sizeof(double2);
   switch (K) {
     case 1: k_lrho<1><<<grid, NT, smem, s>>>(P, x, e, TR, CG); break;

@@ -272,4 +272,13 @@ void launch_lrho_any(const DeviceProgram &P, const double2 *x, const Epi &e, cud
   }
 }
 
+bool launch_lrho_batch(const DeviceProgram &P, const double2 *x, double2 *y, int nbatch, cudaStream_t s) {
+  if (P.has_qubit || nbatch < 1 || nbatch > 65535) return false;  // qubit kernels: one vector per launch
+  Epi e;
+  zero_epi(e);
+  e.kout = y;
+  launch_lrho(P.dev, x, e, s, nbatch);
+  return true;
+}
+
 }  // namespace quac

@@ -48,9 +48,12 @@ __device__ __forceinline__ double2 ldv(const float2 *p) {
 __device__ __forceinline__ void stv(double2 *p, double2 v) { *p = v; }
 __device__ __forceinline__ void stv(float2 *p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
 
-// y[0] += sum_i x[i*(D+1)]  (the stabilising trace row)
+// y[0] += sum_i x[i*(D+1)]  (the stabilising trace row); slice z of a batch
+// works on x + z*D*D and y + z*D*D
 __global__ void k_trace_add(const double2 *__restrict__ x, double2 *__restrict__ y, int64_t D) {
   __shared__ double2 red[NT / 32];
+  x += (size_t)blockIdx.z * D * D;
+  y += (size_t)blockIdx.z * D * D;
   double2 acc = make_double2(0.0, 0.0);
   for (int64_t i = threadIdx.x; i < D; i += NT) {
     const double2 v = x[i * (D + 1)];
@@ -74,10 +77,13 @@ __global__ void k_trace_add(const double2 *__restrict__ x, double2 *__restrict__
 // elements) of conj(V_k[i]) w[i].  The chunk of w is staged in shared
 // memory; each warp then takes one basis vector k = blockIdx.y * 8 + warp,
 // so all projections run side by side (grid nb x ceil(nk / 8)).
+// A batch (gridDim.z > 1) projects w + z*n into partial + z*nk*nb.
 template <typename VT>
 __global__ void k_multidot(const VT *__restrict__ V, const double2 *__restrict__ w, int64_t n,
                            int nk, double2 *__restrict__ partial, int chunk) {
   __shared__ double2 ws[CHUNK];
+  w += (size_t)blockIdx.z * n;
+  partial += (size_t)blockIdx.z * nk * gridDim.x;
   const int64_t i0 = (int64_t)blockIdx.x * chunk;
   const int len = (int)min((int64_t)chunk, n - i0);
   for (int i = threadIdx.x; i < len; i += NT) ws[i] = w[i0 + i];
@@ -490,6 +496,20 @@ k_defl_apply_small(const double2 *__restrict__ AW, const double2 *__restrict__ E
   }
 }
 
+// W[q*n + c*D + r] = U[r,k] conj(U[c,l]) for q = k*kd + l (the stored
+// deflation basis, every column in one launch)
+__global__ void k_defl_formW(const double2 *__restrict__ U, int D, int kd, double2 *__restrict__ W) {
+  const int64_t n = (int64_t)D * D, total = n * kd * kd;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(t / n);
+    const int64_t e = t - (int64_t)q * n;
+    const int c = (int)(e / D), r = (int)(e - (int64_t)c * D);
+    double2 b = U[(size_t)(q % kd) * D + c];
+    b.y = -b.y;
+    W[t] = cmuls(U[(size_t)(q / kd) * D + r], b);
+  }
+}
+
 // Y += (X Z) / 2 for X (D x D) and Z (D x k, k <= KDMAX), both column-major:
 // thread = row r, block column = a segment of XSEG columns of X, segments
 // summed with atomics (Y zeroed by the caller).
@@ -688,14 +708,15 @@ struct Deflation {
   double2 *Id = nullptr, *Ecol = nullptr;  // kd^2 x kd^2 each (assembly of E)
   // small n: W and AW stored (kd^2 x n each) and the multi-dot partials of W^H w
   double2 *W = nullptr, *AW = nullptr, *pw = nullptr;
+  double2 *pe = nullptr;  // kd^4 x nbw multi-dot partials of W^H A W
   int nbw = 0;
   bool stored() const { return W != nullptr; }
   std::vector<std::complex<double>> Uh;  // host copy of U, column-major D x kd
   int cap = 0;                           // kd the buffers were sized for
   void release() {
-    for (double2 *p : {U, Ei, partial, coef, t1, t2, Y, Z, Id, Ecol, W, AW, pw})
+    for (double2 *p : {U, Ei, partial, coef, t1, t2, Y, Z, Id, Ecol, W, AW, pw, pe})
       if (p) cudaFree(p);
-    U = Ei = partial = coef = t1 = t2 = Y = Z = Id = Ecol = W = AW = pw = nullptr;
+    U = Ei = partial = coef = t1 = t2 = Y = Z = Id = Ecol = W = AW = pw = pe = nullptr;
   }
 };
 
@@ -834,6 +855,7 @@ static bool alloc_deflation(const DeviceProgram &PP, int kd, Deflation &F) {
     QCUDA(cudaMalloc(&F.W, (size_t)K2 * n * sizeof(double2)));
     QCUDA(cudaMalloc(&F.AW, (size_t)K2 * n * sizeof(double2)));
     QCUDA(cudaMalloc(&F.pw, (size_t)K2 * F.nbw * sizeof(double2)));
+    QCUDA(cudaMalloc(&F.pe, (size_t)K2 * K2 * F.nbw * sizeof(double2)));
   }
   return !has_error();
 }
@@ -848,13 +870,30 @@ static bool assemble_E(const DeviceProgram &PP, Deflation &F, cudaStream_t s) {
   for (int q = 0; q < K2; q++) hId[(size_t)q * K2 + q] = make_double2(1.0, 0.0);
   QCUDA(cudaMemcpyAsync(F.Id, hId.data(), hId.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
   const int64_t n = (int64_t)F.D * F.D;
-  for (int q = 0; q < K2; q++) {  // small n: W_q and A W_q are kept
-    double2 *wq = F.stored() ? F.W + (size_t)q * n : F.t1;
-    double2 *awq = F.stored() ? F.AW + (size_t)q * n : F.t2;
-    k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, wq, F.U, F.Id + (size_t)q * K2, F.D, kd);
+  // stored basis on a generic program: W in one launch, A W batched, and
+  // E = W^H A W as one batched multi-dot
+  bool batched = false;
+  if (F.stored() && !PP.has_qubit) {
+    k_defl_formW<<<grid_for(n * K2), NT, 0, s>>>(F.U, F.D, kd, F.W);
     count_launch();
-    apply_A(PP, wq, awq, s);
-    defl_project(F, awq, nullptr, F.Ecol + (size_t)q * K2, 0, s);
+    if (launch_lrho_batch(PP, F.W, F.AW, K2, s)) {
+      k_trace_add<<<dim3(1, 1, K2), NT, 0, s>>>(F.W, F.AW, F.D);
+      k_multidot<double2><<<dim3(F.nbw, (K2 + NT / 32 - 1) / (NT / 32), K2), NT, 0, s>>>(F.W, F.AW, n, K2, F.pe,
+                                                                                         256);
+      k_reduce_rows<<<K2 * K2, NT, 0, s>>>(F.pe, F.nbw, F.Ecol, 0);
+      count_launch(3);
+      batched = true;
+    }
+  }
+  if (!batched) {
+    for (int q = 0; q < K2; q++) {  // small n: W_q and A W_q are kept
+      double2 *wq = F.stored() ? F.W + (size_t)q * n : F.t1;
+      double2 *awq = F.stored() ? F.AW + (size_t)q * n : F.t2;
+      k_defl_expand<<<dim3(F.nbx, F.nby), DR, 0, s>>>(nullptr, wq, F.U, F.Id + (size_t)q * K2, F.D, kd);
+      count_launch();
+      apply_A(PP, wq, awq, s);
+      defl_project(F, awq, nullptr, F.Ecol + (size_t)q * K2, 0, s);
+    }
   }
   QCUDA(cudaMemcpyAsync(hE.data(), F.Ecol, hE.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));

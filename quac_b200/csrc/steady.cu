@@ -1053,14 +1053,23 @@ static bool refresh_deflation(const DeviceProgram &PP, const double2 *x, Deflati
 // true residual b - A x in complex128, so with a complex64 basis (FP32
 // inner) the restarts are the iterative refinement that takes the solution
 // to the complex128 tolerance.
+// With a complex64 basis the residual after a restart carries an error of
+// about eps32 * ||H|| * ||y||, which on ill-conditioned systems (||y|| >>
+// ||r||) can exceed what a cycle gains; *stalled is set (and the run
+// returns) when the true residual has not fallen below 0.9x its value
+// STALL_CYCLES restarts earlier, and the caller continues in complex128.
+constexpr int STALL_CYCLES = 20;
+
 template <typename VT>
 static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double rtol, int m, int64_t maxit,
-                         double *final_res, Deflation *def, bool refresh, cudaStream_t s) {
+                         double *final_res, Deflation *def, bool refresh, cudaStream_t s,
+                         bool *stalled = nullptr) {
   const int64_t n = G.n;
   VT *V = G.basis<VT>();
   std::vector<std::complex<double>> H((size_t)(m + 1) * m), cs(m), sn(m), gvec(m + 1), y(m);
   int64_t it = 0;
   double res = 0;
+  std::vector<double> hist;  // true residual at the start of every cycle
   for (int cycle = 0;; cycle++) {
     if (has_error()) break;
     if (def && refresh && cycle > 0) refresh_deflation(PP, x, *def, s);
@@ -1071,6 +1080,11 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
     double beta = norm2(G.t, n, s);
     res = beta;
     if (beta <= rtol || it >= maxit) break;
+    hist.push_back(beta);
+    if (stalled && hist.size() > (size_t)STALL_CYCLES && !(beta < 0.9 * hist[hist.size() - 1 - STALL_CYCLES])) {
+      *stalled = true;
+      break;
+    }
     if (def) {  // x += Q r, and the cycle starts from P r = r - A Q r
       apply_Q(*def, G.t, def->t1, s);
       k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, def->t1, n, 1.0);
@@ -1201,8 +1215,12 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
     const double2 one = make_double2(1.0, 0.0);
     QCUDA(cudaMemcpyAsync(x, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
   }
-  return f32 ? gmres_run<float2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s)
-             : gmres_run<double2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s);
+  if (!f32) return gmres_run<double2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s);
+  bool stalled = false;
+  int64_t its = gmres_run<float2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s, &stalled);
+  if (!stalled || its < 0) return its;
+  const int64_t more = gmres_run<double2>(PP, G, x, rtol, m, maxit - its, final_res, def, refresh, s);
+  return more < 0 ? -1 : its + more;
 }
 
 }  // namespace quac

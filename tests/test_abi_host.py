@@ -164,3 +164,20 @@ def test_error_mode_returns_instead_of_exiting(quac):
     with pytest.raises(q.QuacError):
         q.construct_matrix(qs)  # no operators yet
     qs.destroy()
+
+
+def test_solver_option_setters_validate_on_the_host(quac):
+    """The steady-state and L.x option setters check their arguments before
+    touching any device state; each rejected value leaves the option as it
+    was (a later valid call still succeeds)."""
+    q = quac
+    for setter, good, bad in [(q.set_gmres_precision, (1, 0), (2, -1)),
+                              (q.set_deflation_refresh, (0, 1), (2,)),
+                              (q.set_gmres_restart, (300, 1024, 100), (0, 1025)),
+                              (q.set_hermitian_mode, (0, 1), (3,)),
+                              (q.set_lrho_precision, (1, 0), (2,))]:
+        for v in bad:
+            with pytest.raises(q.QuacError):
+                setter(v)
+        for v in good:
+            setter(v)

@@ -1,5 +1,6 @@
 // Internal definitions shared by the host runtime and the CUDA kernels.
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 #include <complex>
 #include <cstdint>
@@ -140,7 +141,15 @@ struct PassParams {
   PassTerm t[MAXPT];
 };
 
+// A number no other DeviceProgram of this process carries (caches keyed
+// on a program use it rather than the address, which the heap may reuse).
+inline uint64_t next_program_serial() {
+  static std::atomic<uint64_t> c{0};
+  return ++c;
+}
+
 struct DeviceProgram {
+  uint64_t serial = next_program_serial();
   DevProg dev{};
   HostProg host;
   bool has_qubit = false;

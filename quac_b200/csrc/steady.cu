@@ -79,8 +79,8 @@ __global__ void k_trace_add(const double2 *__restrict__ x, double2 *__restrict__
 // so all projections run side by side (grid nb x ceil(nk / 8)).
 // A batch (gridDim.z > 1) projects w + z*n into partial + z*nk*nb.
 template <typename VT>
-__global__ void k_multidot(const VT *__restrict__ V, const double2 *__restrict__ w, int64_t n,
-                           int nk, double2 *__restrict__ partial, int chunk) {
+__device__ __forceinline__ void multidot_body(const VT *__restrict__ V, const double2 *__restrict__ w, int64_t n,
+                                              int nk, double2 *__restrict__ partial, int chunk) {
   __shared__ double2 ws[CHUNK];
   w += (size_t)blockIdx.z * n;
   partial += (size_t)blockIdx.z * nk * gridDim.x;
@@ -105,6 +105,22 @@ __global__ void k_multidot(const VT *__restrict__ V, const double2 *__restrict__
     acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
   }
   if (lane == 0) partial[(size_t)k * gridDim.x + blockIdx.x] = acc;
+}
+
+template <typename VT>
+__global__ void k_multidot(const VT *__restrict__ V, const double2 *__restrict__ w, int64_t n,
+                           int nk, double2 *__restrict__ partial, int chunk) {
+  multidot_body(V, w, n, nk, partial, chunk);
+}
+
+// Graph form: nk = *jp + 1 read on the device (the grid is sized for the
+// longest restart; blocks past nk leave at once).
+template <typename VT>
+__global__ void k_multidot_j(const VT *__restrict__ V, const double2 *__restrict__ w, int64_t n,
+                             const int *__restrict__ jp, double2 *__restrict__ partial, int chunk) {
+  const int nk = *jp + 1;
+  if ((int)blockIdx.y * (NT / 32) >= nk) return;
+  multidot_body(V, w, n, nk, partial, chunk);
 }
 
 // h[k] (+)= sum_b partial[k*nb + b]; one block per k.  accumulate != 0 adds.
@@ -205,9 +221,9 @@ __global__ void k_arnoldi_finish(double2 *__restrict__ h, const double2 *__restr
 // w[i] -= sum_k h_k V_k[i] with CGS_KG k-groups per element, combined in a
 // fixed order.  NORM: npart[block] = sum of |w[i]|^2 over its elements.
 template <typename VT, bool NORM>
-__global__ void __launch_bounds__(CGS_EB * CGS_KG)
-k_cgs_small(const VT *__restrict__ V, const double2 *__restrict__ partial, int nb, int nk, int64_t n,
-            double2 *__restrict__ w, double2 *__restrict__ hout, double *__restrict__ npart) {
+__device__ __forceinline__ void cgs_small_body(const VT *__restrict__ V, const double2 *__restrict__ partial, int nb,
+                                               int nk, int64_t n, double2 *__restrict__ w,
+                                               double2 *__restrict__ hout, double *__restrict__ npart) {
   __shared__ double2 cs[GMRES_MAXM + 1];
   __shared__ double2 red[CGS_KG][CGS_EB];
   __shared__ double nred[CGS_EB / 32 > 0 ? CGS_EB / 32 : 1];
@@ -259,13 +275,32 @@ k_cgs_small(const VT *__restrict__ V, const double2 *__restrict__ partial, int n
   }
 }
 
+template <typename VT, bool NORM>
+__global__ void __launch_bounds__(CGS_EB * CGS_KG)
+k_cgs_small(const VT *__restrict__ V, const double2 *__restrict__ partial, int nb, int nk, int64_t n,
+            double2 *__restrict__ w, double2 *__restrict__ hout, double *__restrict__ npart) {
+  cgs_small_body<VT, NORM>(V, partial, nb, nk, n, w, hout, npart);
+}
+
+// Graph form: step j = *jp; the first pass writes its projections to ring
+// slot j % GMRES_RING of hd (slots of `stride` entries), the second to h2.
+template <typename VT, bool NORM>
+__global__ void __launch_bounds__(CGS_EB * CGS_KG)
+k_cgs_small_j(const VT *__restrict__ V, const double2 *__restrict__ partial, int nb, const int *__restrict__ jp,
+              int64_t n, double2 *__restrict__ w, double2 *__restrict__ hd, int stride, double2 *__restrict__ h2,
+              double *__restrict__ npart) {
+  const int j = *jp;
+  double2 *hout = NORM ? h2 : hd + (size_t)(j % GMRES_RING) * stride;
+  cgs_small_body<VT, NORM>(V, partial, nb, j + 1, n, w, hout, npart);
+}
+
 // Small-n end of an Arnoldi step: every block sums the nparts partial norms
 // (fixed order), block 0 completes the Hessenberg column (hj[k] += h2[k],
 // hj[nk] = ||w||), and all blocks write vnext = w / ||w|| (0 if ||w|| = 0).
 template <typename VT>
-__global__ void k_finish_scale(double2 *__restrict__ hj, const double2 *__restrict__ h2, int nk,
-                               const double *__restrict__ npart, int nparts, const double2 *__restrict__ w,
-                               VT *__restrict__ vnext, int64_t n) {
+__device__ __forceinline__ void finish_scale_body(double2 *__restrict__ hj, const double2 *__restrict__ h2, int nk,
+                                                  const double *__restrict__ npart, int nparts,
+                                                  const double2 *__restrict__ w, VT *__restrict__ vnext, int64_t n) {
   __shared__ double nv;
   if (threadIdx.x < 32) {
     double t = 0.0;
@@ -287,6 +322,34 @@ __global__ void k_finish_scale(double2 *__restrict__ hj, const double2 *__restri
     const double2 v = w[i];
     stv(vnext + i, make_double2(v.x * sc, v.y * sc));
   }
+}
+
+template <typename VT>
+__global__ void k_finish_scale(double2 *__restrict__ hj, const double2 *__restrict__ h2, int nk,
+                               const double *__restrict__ npart, int nparts, const double2 *__restrict__ w,
+                               VT *__restrict__ vnext, int64_t n) {
+  finish_scale_body(hj, h2, nk, npart, nparts, w, vnext, n);
+}
+
+// Graph form: step j = *jp completes ring slot j % GMRES_RING of hd and writes
+// V_{j+1}.
+template <typename VT>
+__global__ void k_finish_scale_j(double2 *__restrict__ hd, int stride, const double2 *__restrict__ h2,
+                                 const int *__restrict__ jp, const double *__restrict__ npart, int nparts,
+                                 const double2 *__restrict__ w, VT *__restrict__ V, int64_t n) {
+  const int j = *jp;
+  finish_scale_body(hd + (size_t)(j % GMRES_RING) * stride, h2, j + 1, npart, nparts, w, V + (size_t)(j + 1) * n, n);
+}
+
+// out = V_j (as complex128) for j = *jp
+template <typename VT>
+__global__ void k_load_vj(const VT *__restrict__ V, const int *__restrict__ jp, int64_t n, double2 *__restrict__ out) {
+  const VT *vj = V + (size_t)(*jp) * n;
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) out[i] = ldv(vj + i);
+}
+
+__global__ void k_step_inc(int *jp) {
+  if (threadIdx.x == 0) *jp += 1;
 }
 
 // out = in * s (s real); also used to copy and convert (s = 1)
@@ -613,6 +676,11 @@ struct Gmres {
   double *npart = nullptr;     // per-block partial norms
   double2 *hh = nullptr;       // pinned host copy of the RING slots
   cudaEvent_t ev[GMRES_RING] = {};
+  // small n: one Arnoldi step as a CUDA graph (step index on the device)
+  int *jdev = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t gkey[6] = {};
+  int64_t gkernels = 0;  // kernels per replay
   int nb = 0, chunk = CHUNK;  // multi-dot partials per projection, elements per partial
   bool small() const { return chunk == 256; }
   template <typename VT> VT *basis() const { return static_cast<VT *>(V); }
@@ -639,18 +707,24 @@ struct Gmres {
     QCUDA(cudaMalloc(&h2, (size_t)(m + 1) * sizeof(double2)));
     QCUDA(cudaMalloc(&npart, (size_t)std::max<int64_t>(grid_for(n), (n + CGS_EB - 1) / CGS_EB) * sizeof(double)));
     QCUDA(cudaMallocHost(&hh, (size_t)GMRES_RING * (m + 2) * sizeof(double2)));
+    QCUDA(cudaMalloc(&jdev, sizeof(int)));
     for (cudaEvent_t &e : ev) QCUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   void release() {
     if (V) {
       cudaFree(V); cudaFree(t); cudaFree(w); cudaFree(partial); cudaFree(h); cudaFree(hd); cudaFree(h2);
       cudaFree(npart);
+      cudaFree(jdev);
       cudaFreeHost(hh);
+      if (gexec) cudaGraphExecDestroy(gexec);
       for (cudaEvent_t &e : ev)
         if (e) cudaEventDestroy(e);
     }
     for (cudaEvent_t &e : ev) e = nullptr;
     V = nullptr;
+    jdev = nullptr;
+    gexec = nullptr;
+    for (uint64_t &k : gkey) k = 0;
     t = w = partial = h = hd = h2 = hh = nullptr;
     npart = nullptr;
     n = 0;
@@ -1053,6 +1127,65 @@ static bool refresh_deflation(const DeviceProgram &PP, const double2 *x, Deflati
 // true residual b - A x in complex128, so with a complex64 basis (FP32
 // inner) the restarts are the iterative refinement that takes the solution
 // to the complex128 tolerance.
+// Captures one small-n Arnoldi step (the step index j lives in G.jdev and
+// every kernel reads it): V_j into t, w = A t (then P w with deflation),
+// the two Gram-Schmidt passes, the Hessenberg column into its ring slot and
+// V_{j+1}; the whole ring of columns is copied to the pinned host ring and
+// j is incremented.  The executable graph is kept for the next step, cycle
+// and solve with the same program, deflation buffers, basis type and
+// restart length.  Returns false (the caller launches the kernels itself)
+// if capture or instantiation fails.
+template <typename VT>
+static bool step_graph(Gmres &G, const DeviceProgram &PP, Deflation *def, int m, cudaStream_t s) {
+  const uint64_t key[6] = {PP.serial, (uint64_t)(uintptr_t)(def ? def->W : nullptr), (uint64_t)(def ? def->kd : 0),
+                           (uint64_t)sizeof(VT), (uint64_t)m, (uint64_t)(uintptr_t)G.V};
+  if (G.gexec && std::equal(key, key + 6, G.gkey)) return true;
+  if (G.gexec) {
+    cudaGraphExecDestroy(G.gexec);
+    G.gexec = nullptr;
+  }
+  const int64_t n = G.n;
+  VT *V = G.basis<VT>();
+  const int nbl = (int)((n + CGS_EB - 1) / CGS_EB);
+  const dim3 gd(G.nb, (m + NT / 32 - 1) / (NT / 32));
+  const int64_t c0 = quac_kernel_launch_count();
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  k_load_vj<<<grid_for(n), NT, 0, s>>>(V, G.jdev, n, G.t);
+  apply_A(PP, G.t, G.w, s);
+  if (def) apply_P(PP, *def, G.w, n, s);
+  k_multidot_j<<<gd, NT, 0, s>>>(V, G.w, n, G.jdev, G.partial, G.chunk);
+  k_cgs_small_j<VT, false><<<nbl, CGS_EB * CGS_KG, 0, s>>>(V, G.partial, G.nb, G.jdev, n, G.w, G.hd, m + 2,
+                                                             G.h2, nullptr);
+  k_multidot_j<<<gd, NT, 0, s>>>(V, G.w, n, G.jdev, G.partial, G.chunk);
+  k_cgs_small_j<VT, true><<<nbl, CGS_EB * CGS_KG, 0, s>>>(V, G.partial, G.nb, G.jdev, n, G.w, G.hd, m + 2,
+                                                            G.h2, G.npart);
+  k_finish_scale_j<<<grid_for(n), NT, 0, s>>>(G.hd, m + 2, G.h2, G.jdev, G.npart, nbl, G.w, V, n);
+  cudaMemcpyAsync(G.hh, G.hd, (size_t)GMRES_RING * (m + 2) * sizeof(double2), cudaMemcpyDeviceToHost, s);
+  k_step_inc<<<1, 32, 0, s>>>(G.jdev);
+  count_launch(7);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+  const int64_t kernels = quac_kernel_launch_count() - c0;
+  count_launch((int)-kernels);  // nothing ran yet; each replay counts them
+  if (ec != cudaSuccess || !graph) {
+    cudaGetLastError();
+    return false;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&G.gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    G.gexec = nullptr;
+    return false;
+  }
+  std::copy(key, key + 6, G.gkey);
+  G.gkernels = kernels;
+  return true;
+}
+
 // With a complex64 basis the residual after a restart carries an error of
 // about eps32 * ||H|| * ||y||, which on ill-conditioned systems (||y|| >>
 // ||r||) can exceed what a cycle gains; *stalled is set (and the run
@@ -1102,7 +1235,15 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
     // only V_j, which step j-1 scaled on the device, so the host queues
     // the next steps before it reads column j back and applies the Givens
     // rotations.  Steps queued past convergence are discarded.
+    const bool graph = G.small() && step_graph<VT>(G, PP, def, m, s);
+    if (graph) QCUDA(cudaMemsetAsync(G.jdev, 0, sizeof(int), s));
     auto launch_step = [&](int j) {
+      if (graph) {  // the step index advances on the device
+        QCUDA(cudaGraphLaunch(G.gexec, s));
+        count_launch((int)G.gkernels);
+        QCUDA(cudaEventRecord(G.ev[j % GMRES_RING], s));
+        return;
+      }
       const VT *vj = V + (size_t)j * n;
       if constexpr (std::is_same<VT, double2>::value) {
         apply_A(PP, reinterpret_cast<const double2 *>(vj), G.w, s);

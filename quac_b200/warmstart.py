@@ -13,11 +13,13 @@ kappa ~ U[0.01, 0.2], gamma ~ U[1e-3, 1e-2], g = 0.1):
    deflation space { u_i u_j^H } from the kd leading left singular vectors
    of F (quac_steady_state_guided), plain GMRES as the fallback.
 
-Deflation only pays when the proposed subspace is close to the true one
-(measured: a neighbour within normalised distance ~0.3 cuts GMRES(100)
-iterations several-fold; one at ~0.6 is worse than no deflation), so the
-guided phase is capped and plain GMRES takes over from its iterate.
-The residual ||(L + e0 vec(I)^T) rho - e0|| <= 1e-11 decides every solve.
+The guided solve projects the deflation space out of the Krylov process
+(Galerkin projection) and, by default, refreshes it at every restart from
+the iterate's leading eigenvectors, so a proposal that is only roughly
+right still converges toward the exact subspace; the proposal's value is
+in the first restarts.  The guided phase is capped and plain GMRES takes
+over from its iterate.  The residual ||(L + e0 vec(I)^T) rho - e0|| <= 1e-11
+decides every solve.
 """
 import time
 

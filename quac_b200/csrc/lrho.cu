@@ -172,6 +172,102 @@ __global__ void __launch_bounds__(NT) k_lrho(const DevProg P, const double2 *__r
   }
 }
 
+// Small systems (D * ncols <= 16384, every partner in L2): S threads share
+// one element.  Lane s takes terms t = s, s + S, ... of every term list, the
+// S partial sums are combined by a butterfly of shuffles (fixed order) and
+// lane 0 applies the same epilogue as k_lrho.  S times more CTAs and S times
+// shorter dependent chains than one thread per element.
+template <int S>
+__global__ void __launch_bounds__(NT) k_lrho_split(const DevProg P, const double2 *__restrict__ X, Epi E) {
+  __shared__ double red[NT / 32];
+  const int D = P.D, NC = P.ncols;
+  if (blockIdx.z) {
+    const size_t zoff = (size_t)blockIdx.z * D * NC;
+    X += zoff;
+    E.kout += zoff;
+  }
+  const int64_t n = (int64_t)D * NC;
+  const int64_t el = ((int64_t)blockIdx.x * NT + threadIdx.x) / S;
+  const int s = threadIdx.x % S;
+  const bool ok = el < n;
+  const int c = ok ? (int)(el / D) : 0;
+  const int r = ok ? (int)(el - (int64_t)c * D) : 0;
+  double2 acc = make_double2(0.0, 0.0);
+  if (ok) {
+    const double2 xs = __ldg(X + el);
+    if (s == 0) {
+      const double2 drr = __ldg(P.dr + r);
+      acc = NC == 1 ? cmul(drr, xs) : cmul(cadd(drr, __ldg(P.dc + c)), xs);
+    }
+    // diagonal jumps: a v(r) conj(v(c)) x[r,c]
+    for (int t = s; t < P.nJd; t += S) {
+      const double2 f = __ldg(P.Jdrow + (size_t)t * D + r);
+      if (f.x == 0.0 && f.y == 0.0) continue;
+      cfma(acc, cmul(f, __ldg(P.Jdcol + (size_t)t * D + c)), xs);
+    }
+    // left Hamiltonian terms: -i a G[r,p] x[p,c]
+    for (int t = s; t < P.nL; t += S) {
+      const int p = __ldg(P.Lmap + (size_t)t * D + r);
+      if (p < 0) continue;
+      cfma(acc, __ldg(P.Lval + (size_t)t * D + r), __ldg(X + (size_t)c * D + p));
+    }
+    // right Hamiltonian terms: +i a x[r,q] G[q,c]
+    for (int t = s; t < P.nR; t += S) {
+      const int q = __ldg(P.Rmap + (size_t)t * D + c);
+      if (q < 0) continue;
+      cfma(acc, __ldg(P.Rval + (size_t)t * D + c), __ldg(X + (size_t)q * D + r));
+    }
+    // jumps: a v(r) conj(v(c)) x[j(r), j(c)]
+    for (int t = s; t < P.nJ; t += S) {
+      const int p = __ldg(P.Jmap + (size_t)t * D + r);
+      if (p < 0) continue;
+      const int q = __ldg(P.Jmap + (size_t)t * D + c);
+      if (q < 0) continue;
+      const double2 f = cmul(__ldg(P.Jrow + (size_t)t * D + r), __ldg(P.Jcol + (size_t)t * D + c));
+      cfma(acc, f, __ldg(X + (size_t)q * D + p));
+    }
+  }
+#pragma unroll
+  for (int o = S / 2; o > 0; o >>= 1) {  // every lane of the group ends with the same sum
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+  }
+  double nloc = 0.0;
+  if (ok && s == 0) {
+    const size_t i = (size_t)el;
+    const double2 Kv = acc;
+    if (E.kout) E.kout[i] = Kv;
+    double2 upd[3];
+#pragma unroll
+    for (int u = 0; u < 3; u++) {
+      if (u < E.nupd) {
+        double2 b = E.base[u] ? E.base[u][i] : make_double2(0.0, 0.0);
+        b.x = fma(E.coef[u], Kv.x, b.x);
+        b.y = fma(E.coef[u], Kv.y, b.y);
+        E.out[u][i] = b;
+        upd[u] = b;
+      }
+    }
+    if (E.nsum) {
+      const double2 e = upd[E.err_upd];
+      const double2 y = E.ny[i];
+      const double2 yn = E.yn_upd >= 0 ? upd[E.yn_upd] : E.nyn[i];
+      const double qv = cabs2(e) / (E.atol + E.rtol * fmax(cabs2(y), cabs2(yn)));
+      nloc = qv * qv;
+    }
+  }
+  if (E.nsum) {
+    for (int o = 16; o > 0; o >>= 1) nloc += __shfl_down_sync(0xffffffffu, nloc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nloc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; w++) t += red[w];
+      atomicAdd(E.nsum, t);
+    }
+  }
+}
+
 }  // namespace
 
 void ensure_smem(const void *func, size_t bytes) {
@@ -203,9 +299,15 @@ void launch_lrho(const DevProg &P, const double2 *x, const Epi &e, cudaStream_t 
     CG = NT / TR;
     K = 8;
     while (K > 1 && (int64_t)CG * (K / 2) >= P.ncols) K /= 2;
-    // small systems: one column per thread, so the few CTAs there are
-    // split the work as finely as they can
-    if ((int64_t)P.D * P.ncols <= (int64_t)NT * 64) K = 1;
+  }
+  // small systems: several threads per element (k_lrho_split)
+  if ((int64_t)P.D * P.ncols <= (int64_t)NT * 64) {
+    constexpr int S = 8;
+    const int64_t threads = (int64_t)P.D * P.ncols * S;
+    k_lrho_split<S><<<dim3((unsigned)((threads + NT - 1) / NT), 1, nbatch), NT, 0, s>>>(P, x, e);
+    count_launch();
+    QCUDA(cudaGetLastError());
+    return;
   }
   const int TC = CG * K;
   dim3 grid((P.D + TR - 1) / TR, (P.ncols + TC - 1) / TC, nbatch);

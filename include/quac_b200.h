@@ -349,10 +349,14 @@ void quac_clear_error(void);
  * adapt "basic" | "none"; non-positive tolerances keep the current ones. */
 int quac_set_ts_options(const char *rk_type, const char *adapt_type, double rtol, double atol,
                         PetscInt max_steps);
-/* Device pointer of a qvec (complex128, qvec->n values). */
+/* Device pointer of a qvec (complex128, qvec->n values).  Work the caller
+ * queues on it must be ordered with the system's stream (the one given to
+ * quac_set_stream, or synchronise first): time_step_sys and the other
+ * calls wait only on their own stream. */
 void *quac_qvec_device_ptr(qvec q);
 /* Launch this system's kernels on a caller-owned CUDA stream (NULL: the
- * library's own stream). */
+ * library's own stream).  Calls return when their work on that stream is
+ * done. */
 void quac_set_stream(qsystem qsys, void *cuda_stream);
 /* Kernel selection for systems compiled afterwards: 0 = default (multi-pass
  * bit-mask kernel for all-qubit systems of seven or more qubits, single-pass

@@ -482,6 +482,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 16 * n},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "frac_of_nominal_8tbs": achieved / 8000.0,
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                      "kernel": "Hermitian mode: k_qpass_hh (high-qubit pass, upper triangle of each "
                                "tile) then k_qpass (low-qubit pass on the blocks I <= J with the fused RK "

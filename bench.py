@@ -376,8 +376,8 @@ def steady_summary(q):
     from e0 against the learned start (FP32-inner / FP64-refined GMRES(300),
     deflation refreshed every restart), and the same solver without the
     network."""
-    from quac_b200 import steady_probe
-    out = steady_probe.run_sweep(q, steady_probe.defaults(sweep2d=True, restart=300))
+    from quac_b200 import warmstart
+    out = warmstart.measure_sweep(q, warmstart.sweep_settings(sweep2d=True, restart=300))
     return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "solver", "cold", "method",
                                 "learned", "learned_vs_cold", "learned_vs_method", "method_vs_cold",
                                 "pop_err_max", "residual_max")}
@@ -411,25 +411,6 @@ def run_ours(args, rank, world, local_rank):
         q.time_step_sys(qs, rho, t, t + RK_STEPS * DT, DT, 10 ** 9)
 
     t = 0.0
-    # Settle: on freshly acquired boxes this kernel has run 3-5x slower for
-    # stretches of seconds at normal clocks and normal copy bandwidth (cause
-    # outside this process).  Untimed segments run until three in a row agree
-    # within 5 % and are within 1.3x of the fastest seen, for at most 60 s;
-    # the W warm-up steps and the timed K steps follow.
-    settle_t0, times = time.perf_counter(), []
-    while time.perf_counter() - settle_t0 < 60.0:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        segment(t)
-        e1.record(stream)
-        e1.synchronize()
-        t += RK_STEPS * DT
-        times.append(e0.elapsed_time(e1))
-        last = times[-3:]
-        if len(last) == 3 and max(last) <= 1.05 * min(last) and max(last) <= 1.3 * min(times):
-            break
-    settle = {"seconds": time.perf_counter() - settle_t0, "segments": len(times),
-              "first_ms": times[0], "last_ms": times[-1]}
     for _ in range(args.warmup):
         segment(t)
         t += RK_STEPS * DT
@@ -442,15 +423,19 @@ def run_ours(args, rank, world, local_rank):
     launches0 = q.kernel_launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    seg_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     torch.cuda.synchronize()
     ev0.record(stream)
-    for _ in range(args.steps):
+    for k in range(args.steps):
+        seg_ev[k].record(stream)
         segment(t)
         t += RK_STEPS * DT
+    seg_ev[args.steps].record(stream)
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = q.kernel_launch_count() - launches0
     ms = ev0.elapsed_time(ev1)
+    seg_ms = [seg_ev[k].elapsed_time(seg_ev[k + 1]) for k in range(args.steps)]
     clk = clocks.stop()
     # e2e through the C ABI with host (pinned) buffers
     host = torch.from_numpy(x0.copy()).pin_memory()
@@ -484,13 +469,13 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / peak, "traffic": traffic,
                      "frac_of_nominal_8tbs": achieved / 8000.0,
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-                     "kernel": "Hermitian mode: k_qpass_hh (high-qubit pass, upper triangle of each "
-                               "tile) then k_qpass (low-qubit pass on the blocks I <= J with the fused RK "
-                               "stage epilogue and conjugate-transposed writes)",
+                     "kernel": "Hermitian mode: k_qpass over tile pairs (a <= b) of the high-qubit pass, "
+                               "then k_qpass over the blocks I <= J of the low-qubit pass with the fused RK "
+                               "stage epilogue and conjugate-transposed writes",
                      "per": "one L.rho application (32*D^2 algorithmic bytes)"},
         "gpu_launches": int(launches),
         "clocks": clk,
-        "settle": settle,
+        "segment_ms": {"min": min(seg_ms), "median": statistics.median(seg_ms), "max": max(seg_ms)},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
@@ -508,6 +493,86 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
+def run_profile(args):
+    """Small cases of single kernels for profiler captures (no JSON line):
+
+      --profile lrho     --qubits N --reps R [--fp32] [--path P]   L.x applications on device buffers
+      --profile rk4      --qubits N --rk4-steps K [--fp32]         fixed RK4 from a Hermitian state
+                                                                     (Hermitian mode of the pass kernel)
+      --profile ensemble --instances N --t-end T [--fp32]          one persistent ensemble launch
+      --profile gemm     --m M --n N --k K --reps R                 TF32 tensor-core GEMM
+      --profile steady   --ne E --nc C --train T --held H --kd K --restart M --fp32-basis B --sweep2d
+                                                                     learned warm-start sweep
+    """
+    import ctypes
+    import torch
+    import quac_b200 as q
+    from quac_b200 import systems as Sy
+    q.lib()
+    q.QuaC_initialize()
+    q.set_lrho_precision(1 if args.fp32 else 0)
+    if args.profile in ("lrho", "rk4"):
+        q.set_kernel_path(args.path)
+        S = Sy.Builder(q)
+        tfim_terms(S, n=args.qubits)
+        q.construct_matrix(S.qs)
+        D = S.D
+        if args.profile == "rk4":
+            X = torch.randn(D, D, dtype=torch.complex128)
+            X = (X + X.conj().T) / 2
+            rho = q.create_dm_sys(S.qs)
+            rho.from_numpy(X.T.contiguous().reshape(-1).numpy())  # column-stacked
+            q.set_ts_options(rk_type="4", adapt_type="none")
+            q.time_step_sys(S.qs, rho, 0.0, DT * args.rk4_steps, DT, 10 ** 6)
+            torch.cuda.synchronize()
+            print(f"ok D={D} rk4 steps={args.rk4_steps} hermitian applications={q.hermitian_apply_count()}")
+            return
+        x = torch.randn(D * D, dtype=torch.complex128, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(args.reps):
+            q.lrho_apply_device(S.qs, x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        print(f"ok D={D} reps={args.reps} launches={q.kernel_launch_count()}")
+    elif args.profile == "ensemble":
+        params = Sy.driven_jc_ensemble_params(args.instances)
+        built = []
+        for p in params:
+            B = Sy.Builder(q)
+            Sy.driven_jc(B, **p)
+            built.append(B.qs)
+        E = q.Ensemble(built)
+        E.set_options(precision=1 if args.fp32 else 0)
+        E.set_states(np.concatenate([Sy.excited_vacuum(p["nc"]) for p in params]))
+        t0 = time.perf_counter()
+        E.run(0.0, args.t_end, 0.05)
+        print(f"ok {args.instances} instances to t={args.t_end} in {(time.perf_counter() - t0) * 1e3:.1f} ms")
+        E.destroy()
+    elif args.profile == "gemm":
+        L = q.lib()
+        L.quac_gemm_tf32.restype = ctypes.c_int
+        L.quac_gemm_tf32.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int] * 4
+        A = torch.randn(args.m, args.k, device="cuda")
+        Bm = torch.randn(args.n, args.k, device="cuda")
+        bias = torch.randn(args.n, device="cuda")
+        C = torch.empty(args.m, args.n, device="cuda")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for i in range(args.reps):
+            if i == args.reps - 1:
+                ev0.record()
+            assert L.quac_gemm_tf32(A.data_ptr(), Bm.data_ptr(), C.data_ptr(), bias.data_ptr(),
+                                    args.m, args.n, args.k, 0) == 0
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        print(f"ok {args.m}x{args.n}x{args.k}: {ms * 1e3:.1f} us per GEMM, "
+              f"{2.0 * args.m * args.n * args.k / ms / 1e9:.1f} TFLOP/s")
+    elif args.profile == "steady":
+        from quac_b200 import warmstart
+        a = warmstart.sweep_settings(ne=args.ne, nc=args.nc, train=args.train, held=args.held, kd=args.kd,
+                                     restart=args.restart, fp32=args.fp32_basis, sweep2d=args.sweep2d)
+        print(json.dumps(warmstart.measure_sweep(q, a)))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -517,7 +582,30 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the sections beside the headline (complex64, ensemble, JC, circuit, steady state)")
+    ap.add_argument("--profile", choices=["lrho", "rk4", "ensemble", "gemm", "steady"],
+                    help="run one small case for a profiler capture instead of the benchmark")
+    ap.add_argument("--qubits", type=int, default=NQ)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--path", type=int, default=0)
+    ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--rk4-steps", type=int, default=2)
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--t-end", type=float, default=2.0)
+    ap.add_argument("--m", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--k", type=int, default=4096)
+    ap.add_argument("--ne", type=int, default=3)
+    ap.add_argument("--nc", type=int, default=4)
+    ap.add_argument("--train", type=int, default=48)
+    ap.add_argument("--held", type=int, default=12)
+    ap.add_argument("--kd", type=int, default=8)
+    ap.add_argument("--restart", type=int, default=300)
+    ap.add_argument("--fp32-basis", type=int, default=1)
+    ap.add_argument("--sweep2d", action="store_true")
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -174,6 +174,22 @@ void add_ham_term(qsystem qsys, PetscScalar a, PetscInt num_ops, ...); /* qsyste
 void add_lin_term(qsystem qsys, PetscScalar a, PetscInt num_ops, ...); /* qsystem.c:436-462 */
 void add_lin_term_list(qsystem qsys, PetscScalar a, PetscInt num_ops, op_handle *ops); /* qsystem.c:464-489 */
 void add_ham_term_list(qsystem qsys, PetscScalar a, PetscInt num_ops, op_handle *ops); /* list form of qsystem.c:407-434 */
+/* Time-dependent terms: qsystem.h:31-32, qsystem.c:491-552.  The term's
+ * superoperator is built with coefficient 1 and scaled at every stage time
+ * t by a * f(t, ctx) (the reference calls f with the time and ctx,
+ * qsystem.c:1311-1316, although its header prints a one-argument type);
+ * terms whose |a f(t)| is at most 1e-10 are skipped at that stage
+ * (qsystem.c:1320).  add_lin_term_time_dep selects the density-matrix
+ * equations like add_lin_term. */
+typedef PetscScalar (*quac_time_dep_func)(PetscReal t, void *ctx);
+void add_ham_term_time_dep(qsystem qsys, PetscScalar a, void *ctx, quac_time_dep_func f, PetscInt num_ops, ...);
+void add_lin_term_time_dep(qsystem qsys, PetscScalar a, void *ctx, quac_time_dep_func f, PetscInt num_ops, ...);
+/* List forms of the two (kind 1 = Hamiltonian, 2 = Lindblad) for callers
+ * whose callbacks cannot return a complex value (language bindings):
+ * g(t, ctx, &re, &im) writes f(t). */
+typedef void (*quac_time_dep_func_parts)(PetscReal t, void *ctx, double *re, double *im);
+int quac_add_term_time_dep_list(qsystem qsys, int kind, PetscScalar a, void *ctx, quac_time_dep_func_parts g,
+                                PetscInt num_ops, op_handle *ops);
 void clear_mat_terms_sys(qsystem qsys);                 /* qsystem.c:557-591 */
 void construct_matrix(qsystem qsys);                    /* qsystem.c:593-676 */
 void use_mcwf_solver(qsystem qsys, PetscInt num_tot_trajs, PetscInt seed); /* qsystem.c:358-403 */
@@ -231,6 +247,17 @@ void add_lin(PetscScalar a, op_handle op);              /* operators.c:679-719 *
 void add_lin_mult2(PetscScalar a, op_handle op1, op_handle op2);      /* operators.c:743-821 */
 void steady_state(Vec x);                               /* solver.c:33-221 */
 void set_ts_monitor(quac_ts_monitor monitor);           /* solver.c:526-532 */
+void create_full_dm(Vec *dm);                           /* dm_utilities.c:635-655 */
+void create_dm(Vec *dm, PetscInt size);                 /* dm_utilities.c:616-623 */
+void destroy_dm(Vec dm);                                /* dm_utilities.c:1029-1032 */
+void add_value_to_dm(Vec dm, PetscInt row, PetscInt col, PetscScalar val); /* dm_utilities.c:1049-1061 */
+void assemble_dm(Vec dm);                               /* dm_utilities.c:1073-1076 */
+void get_dm_element(Vec dm, PetscInt row, PetscInt col, PetscScalar *val); /* dm_utilities.c:965-982 */
+int get_num_populations(void);                          /* dm_utilities.c:1127-1143 */
+/* dm_utilities.c:1157-1325: per subsystem of the legacy system, Tr(n rho);
+ * a VEC subsystem gives one population per level.  *populations must hold
+ * get_num_populations() doubles. */
+void get_populations(Vec x, double **populations);
 
 /* --------------------------------------------- PETSc Vec/TS stand-ins */
 PetscErrorCode VecGetArray(Vec v, PetscScalar **a);     /* maps the data to host memory */
@@ -262,8 +289,12 @@ int quac_lrho_apply_host(qsystem qsys, const PetscScalar *x_host, PetscScalar *y
  * fixed 16 MiB device array, so qsys->dim may be at most 2^20 (10 qubits);
  * larger systems return an error.  Call quac_lrho_noalloc_setup(qsys) once,
  * with the system's device current, before the first apply and before any
- * stream capture.  All systems on a device share the one array: calls that
- * overlap in time race and must be serialised by the caller. */
+ * stream capture: it may allocate (the system's term tables) and loads every
+ * kernel the apply can launch, so that the apply itself allocates nothing.
+ * The apply computes in the precision quac_set_lrho_precision selects, like
+ * quac_lrho_apply_device, and returns once y is complete.  All systems on a
+ * device share the one array: calls that overlap in time race and must be
+ * serialised by the caller. */
 int quac_lrho_noalloc_setup(qsystem qsys);
 int quac_lrho_apply_device_noalloc(qsystem qsys, const void *x_dev, void *y_dev);
 /* Batched ensembles (no reference counterpart: QuaC integrates one system
@@ -371,12 +402,13 @@ void quac_set_kernel_path(int path);
  * reduction kept in complex128.  Other kernels always run complex128. */
 int quac_set_lrho_precision(int precision);
 /* Hermitian mode of time_step_sys (no reference counterpart): 1 (default) =
- * automatic: for a 12-qubit system on the multi-pass kernel whose terms
- * preserve Hermiticity, integrated from a Hermitian state with no gate
- * events inside the run, every L.x computes the blocks on and above the
- * block diagonal only and writes the others as their conjugate transposes
- * (half the outputs and most of the traffic); 0 = always compute every
- * element. */
+ * automatic: for a system of 7 or more qubits on the multi-pass kernel whose
+ * terms preserve Hermiticity, integrated from a Hermitian state with no gate
+ * events inside the run, every L.x computes the 64 x 64 blocks on and above
+ * the block diagonal only and writes the others as their conjugate
+ * transposes (half the outputs and a third of the traffic); 2 = the same,
+ * and also in quac_lrho_apply_device / quac_lrho_apply_host when x is
+ * Hermitian to 1e-13; 0 = always compute every element. */
 int quac_set_hermitian_mode(int mode);
 /* Restart length of the steady-state GMRES (default 100 as in solver.c;
  * -ksp_gmres_restart on the QuaC_initialize command line does the same).

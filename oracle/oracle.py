@@ -181,6 +181,32 @@ def rk4(h, y0, dt, nsteps):
     return y
 
 
+def rk4_time_dep(h0, terms, y0, t0, dt, nsteps, min_time_dep=1e-10):
+    """Classical RK4 on Y = A X + sum_k a_k f_k(t) A_k X, the matrix-shell
+    product of qsystem.c:1300-1330: `h0` is the CSR of the time-independent
+    terms, `terms` a list of (csr handle of the term built with coefficient
+    1, a_k, f_k); a term whose |a_k f_k(t)| is at most min_time_dep
+    (qsystem.c:34) is skipped at that time."""
+    def rhs(t, x):
+        y = spmv(h0, x)
+        for hk, a, f in terms:
+            s = a * f(t)
+            if abs(s) > min_time_dep:
+                y = y + s * spmv(hk, x)
+        return y
+
+    y = np.array(y0, dtype=np.complex128, copy=True)
+    t = t0
+    for _ in range(nsteps):
+        k1 = rhs(t, y)
+        k2 = rhs(t + dt / 2, y + dt / 2 * k1)
+        k3 = rhs(t + dt / 2, y + dt / 2 * k2)
+        k4 = rhs(t + dt, y + dt * k3)
+        y = y + dt / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+        t = t0 + (_ + 1) * dt
+    return y
+
+
 def bs3(h, y0, t0, tmax, dt0, atol=5e-7, rtol=5e-7, hmin=0.01, hmax=1.0, max_steps=10 ** 9):
     y = np.array(y0, dtype=np.complex128, copy=True)
     nrej = ctypes.c_int64(0)

@@ -200,6 +200,27 @@ def lib():
         "quac_ensemble_run": (ctypes.c_int, [vp, dbl, dbl, dbl]),
         "quac_ensemble_get_stats": (ctypes.c_int, [vp, i64, P(dbl), P(i64), P(i64), P(ctypes.c_int)]),
         "quac_ensemble_populations": (ctypes.c_int, [vp, vp]),
+        "create_op": (None, [ctypes.c_int, P(_OpPtr)]),
+        "create_vec": (None, [ctypes.c_int, P(P(_OpPtr))]),
+        "add_to_ham": (None, [Scalar, _OpPtr]),
+        "add_to_ham_mult2": (None, [Scalar, _OpPtr, _OpPtr]),
+        "add_to_ham_mult3": (None, [Scalar, _OpPtr, _OpPtr, _OpPtr]),
+        "add_lin": (None, [Scalar, _OpPtr]),
+        "add_lin_mult2": (None, [Scalar, _OpPtr, _OpPtr]),
+        "steady_state": (None, [vp]),
+        "create_full_dm": (None, [P(vp)]),
+        "create_dm": (None, [P(vp), i64]),
+        "destroy_dm": (None, [vp]),
+        "add_value_to_dm": (None, [vp, i64, i64, Scalar]),
+        "assemble_dm": (None, [vp]),
+        "get_dm_element": (None, [vp, i64, i64, P(Scalar)]),
+        "get_num_populations": (ctypes.c_int, []),
+        "get_populations": (None, [vp, P(P(dbl))]),
+        "VecGetArray": (ctypes.c_int, [vp, P(P(Scalar))]),
+        "VecRestoreArray": (ctypes.c_int, [vp, P(P(Scalar))]),
+        "get_bitstring_probs": (None, [P(_QvecStruct), P(i64), P(P(dbl)), P(P(dbl))]),
+        "quac_add_term_time_dep_list": (ctypes.c_int, [P(_QsysStruct), ctypes.c_int, Scalar, vp, vp, i64,
+                                                       P(_OpPtr)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -417,6 +438,36 @@ def add_ham_term(qs, a, *ops):
 def add_lin_term(qs, a, *ops):
     lib().add_lin_term_list(qs._ptr, _sc(a), len(ops), _oplist(ops))
     _check()
+
+
+_TdFn = ctypes.CFUNCTYPE(None, ctypes.c_double, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(ctypes.c_double))
+
+
+def _add_td(qs, kind, a, fn, ops):
+    def _cb(t, ctx, re, im):
+        v = complex(fn(t))
+        re[0] = v.real
+        im[0] = v.imag
+
+    cb = _TdFn(_cb)
+    if not hasattr(qs, "_td_callbacks"):
+        qs._td_callbacks = []
+    qs._td_callbacks.append(cb)  # kept alive as long as the system
+    arr = _oplist(ops)
+    lib().quac_add_term_time_dep_list(qs._ptr, kind, _sc(a), None, ctypes.cast(cb, vp), len(ops), arr)
+    _check()
+
+
+def add_ham_term_time_dep(qs, a, fn, *ops):
+    """Hamiltonian term a f(t) ops[0] ops[1] ... (qsystem.c:491-519); fn(t)
+    returns a number."""
+    _add_td(qs, 1, a, fn, ops)
+
+
+def add_lin_term_time_dep(qs, a, fn, *ops):
+    """Lindblad term with rate a f(t) (qsystem.c:521-552)."""
+    _add_td(qs, 2, a, fn, ops)
 
 
 def clear_mat_terms_sys(qs):
@@ -700,7 +751,8 @@ def set_deflation_refresh(mode):
 
 
 def set_hermitian_mode(mode):
-    """1 (default): Hermitian mode when it applies; 0: never."""
+    """1 (default): Hermitian mode in time_step_sys when it applies; 2: also
+    in the single L.x entry points for a Hermitian input; 0: never."""
     lib().quac_set_hermitian_mode(int(mode))
     _check()
 
@@ -868,3 +920,132 @@ class WarmStartNet:
         if self._h:
             lib().quac_wsnet_destroy(self._h)
             self._h = None
+
+
+# ------------------------------------------------ legacy global-system API
+# (operators.c, dm_utilities.c, solver.c): one implicit system built with
+# create_op / add_to_ham / add_lin, density matrices as bare Vec handles
+
+class LegacyVec:
+    """A Vec of the legacy API (device vector handle)."""
+
+    def __init__(self, ptr):
+        self._ptr = ptr
+
+    def size(self):
+        n = ctypes.c_int64()
+        lib().VecGetSize(self._ptr, ctypes.byref(n))
+        return n.value
+
+    def to_numpy(self):
+        a = ctypes.POINTER(Scalar)()
+        lib().VecGetArray(self._ptr, ctypes.byref(a))
+        n = self.size()
+        out = np.ctypeslib.as_array(ctypes.cast(a, ctypes.POINTER(ctypes.c_double)), shape=(2 * n,)).copy()
+        lib().VecRestoreArray(self._ptr, ctypes.byref(a))
+        return out[0::2] + 1j * out[1::2]
+
+    def destroy(self):
+        if self._ptr:
+            lib().destroy_dm(self._ptr)
+            self._ptr = None
+
+
+def create_op(levels):
+    p = _OpPtr()
+    lib().create_op(int(levels), ctypes.byref(p))
+    _check()
+    return Operator(p)
+
+
+def add_to_ham(a, op):
+    lib().add_to_ham(_sc(a), op._ptr)
+    _check()
+
+
+def add_to_ham_mult2(a, op1, op2):
+    lib().add_to_ham_mult2(_sc(a), op1._ptr, op2._ptr)
+    _check()
+
+
+def add_lin(a, op):
+    lib().add_lin(_sc(a), op._ptr)
+    _check()
+
+
+def add_lin_mult2(a, op1, op2):
+    lib().add_lin_mult2(_sc(a), op1._ptr, op2._ptr)
+    _check()
+
+
+def create_full_dm():
+    p = ctypes.c_void_p()
+    lib().create_full_dm(ctypes.byref(p))
+    _check()
+    return LegacyVec(p)
+
+
+def add_value_to_dm(dm, row, col, val):
+    lib().add_value_to_dm(dm._ptr, int(row), int(col), _sc(val))
+    _check()
+
+
+def assemble_dm(dm):
+    lib().assemble_dm(dm._ptr)
+    _check()
+
+
+def get_dm_element(dm, row, col):
+    s = Scalar()
+    lib().get_dm_element(dm._ptr, int(row), int(col), ctypes.byref(s))
+    _check()
+    return complex(s.re, s.im)
+
+
+def steady_state(dm):
+    """solver.c:33-221 on the legacy system, result in dm."""
+    lib().steady_state(dm._ptr)
+    _check()
+
+
+def get_populations(dm):
+    n = lib().get_num_populations()
+    out = (ctypes.c_double * n)()
+    p = ctypes.cast(out, ctypes.POINTER(ctypes.c_double))
+    lib().get_populations(dm._ptr, ctypes.byref(p))
+    _check()
+    return np.array(out[:])
+
+
+def get_bitstring_probs(q):
+    """Probabilities of the computational basis states (the diagonal of
+    rho, or |psi_i|^2), as get_bitstring_probs returns them."""
+    n = ctypes.c_int64()
+    pr, va = ctypes.POINTER(ctypes.c_double)(), ctypes.POINTER(ctypes.c_double)()
+    lib().get_bitstring_probs(q._ptr, ctypes.byref(n), ctypes.byref(pr), ctypes.byref(va))
+    _check()
+    out = np.ctypeslib.as_array(pr, shape=(n.value,)).copy()
+    libc = ctypes.CDLL(None)
+    libc.free.argtypes = [ctypes.c_void_p]
+    libc.free(ctypes.cast(pr, ctypes.c_void_p))
+    libc.free(ctypes.cast(va, ctypes.c_void_p))
+    return out
+
+
+def read_qvec_dm_binary(path):
+    p = ctypes.POINTER(_QvecStruct)()
+    lib().read_qvec_dm_binary(ctypes.byref(p), os.fsencode(path))
+    _check()
+    return Qvec(p)
+
+
+def read_qvec_wf_binary(path):
+    p = ctypes.POINTER(_QvecStruct)()
+    lib().read_qvec_wf_binary(ctypes.byref(p), os.fsencode(path))
+    _check()
+    return Qvec(p)
+
+
+def print_qvec_file(q, path):
+    lib().print_qvec_file(q._ptr, os.fsencode(path))
+    _check()

@@ -251,6 +251,8 @@ void initialize_system(qsystem *qsys) {
 
 void clear_mat_terms_sys(qsystem qs) {
   qs->impl->terms.clear();
+  release_td_programs(qs);
+  qs->impl->td.clear();
   if (qs->impl->prog) {
     qs->impl->prog->release();
     delete qs->impl->prog;
@@ -430,6 +432,49 @@ void add_ham_term_list(qsystem qs, PetscScalar a, PetscInt num_ops, op_handle *o
   record_term(qs, 1, a, num_ops, ops);
 }
 
+static void record_td_term(qsystem qs, int kind, PetscScalar a, void *ctx, quac_time_dep_func f,
+                           quac_time_dep_func_parts g, PetscInt num_ops, op_handle *ops) {
+  if (!f && !g) { fail(9, "ERROR! NULL time-dependence function passed to a time-dependent term\n"); return; }
+  TdTerm td;
+  td.term.kind = kind;
+  td.term.a = cplx(PetscRealPart(a), PetscImaginaryPart(a));
+  for (PetscInt i = 0; i < num_ops; i++) {
+    if (!ops[i]) { fail(9, "ERROR! NULL operator passed to a term\n"); return; }
+    td.term.ops.push_back(ops[i]);
+  }
+  td.f = f;
+  td.g = g;
+  td.ctx = ctx;
+  if (kind == 2) qs->dm_equations = PETSC_TRUE;  // qsystem.c:531
+  qs->impl->td.push_back(td);
+  qs->num_time_dep = (PetscInt)qs->impl->td.size();
+}
+
+void add_ham_term_time_dep(qsystem qs, PetscScalar a, void *ctx, quac_time_dep_func f, PetscInt num_ops, ...) {
+  std::vector<op_handle> ops(num_ops);
+  va_list ap;
+  va_start(ap, num_ops);
+  for (PetscInt i = 0; i < num_ops; i++) ops[i] = va_arg(ap, op_handle);
+  va_end(ap);
+  record_td_term(qs, 1, a, ctx, f, nullptr, num_ops, ops.data());
+}
+
+void add_lin_term_time_dep(qsystem qs, PetscScalar a, void *ctx, quac_time_dep_func f, PetscInt num_ops, ...) {
+  std::vector<op_handle> ops(num_ops);
+  va_list ap;
+  va_start(ap, num_ops);
+  for (PetscInt i = 0; i < num_ops; i++) ops[i] = va_arg(ap, op_handle);
+  va_end(ap);
+  record_td_term(qs, 2, a, ctx, f, nullptr, num_ops, ops.data());
+}
+
+int quac_add_term_time_dep_list(qsystem qs, int kind, PetscScalar a, void *ctx, quac_time_dep_func_parts g,
+                                PetscInt num_ops, op_handle *ops) {
+  if (kind != 1 && kind != 2) { fail(0, "ERROR! term kind must be 1 (Hamiltonian) or 2 (Lindblad)\n"); return 1; }
+  record_td_term(qs, kind, a, ctx, nullptr, g, num_ops, ops);
+  return has_error() ? 1 : 0;
+}
+
 void use_mcwf_solver(qsystem qs, PetscInt num_tot_trajs, PetscInt seed) {
   (void)qs; (void)num_tot_trajs; (void)seed;
   fail(9, "ERROR! use_mcwf_solver: the Monte-Carlo wavefunction solver is not provided by this engine\n");
@@ -441,7 +486,7 @@ void construct_matrix(qsystem qs) {
     fail(0, "ERROR! You need to create operators before you construct\n       a matrix!\n");
     return;
   }
-  if (qs->impl->terms.empty()) {
+  if (qs->impl->terms.empty() && qs->impl->td.empty()) {
     fail(0, "ERROR! You need to add some terms before you construct\n       a matrix!\n");
     return;
   }
@@ -1129,6 +1174,78 @@ void steady_state(Vec x) {
   if (its >= 0) printf("Iterations %ld\n", (long)its);
 }
 
+// legacy density-matrix helpers (dm_utilities.c): the Vec holds the
+// column-stacked density matrix of the legacy system
+void create_full_dm(Vec *dm) {
+  qsystem qs = legacy();
+  const int64_t D = qs->total_levels;
+  *dm = vec_new(qs->dm_equations ? D * D : D);
+}
+
+void create_dm(Vec *dm, PetscInt size) { *dm = vec_new((int64_t)size * size); }
+
+void destroy_dm(Vec dm) { vec_free(dm); }
+
+static int64_t dm_side(Vec v) { return (int64_t)std::llround(std::sqrt((double)v->n)); }
+
+void add_value_to_dm(Vec dm, PetscInt row, PetscInt col, PetscScalar val) {
+  // like the reference on one rank: a location outside the vector is not stored
+  const int64_t loc = dm_side(dm) * col + row;
+  if (loc < 0 || loc >= dm->n) return;
+  if (!dm->host_pending) vec_pull_host(dm);
+  dm->host_pending = true;
+  dm->h[loc] += cplx(PetscRealPart(val), PetscImaginaryPart(val));
+}
+
+void assemble_dm(Vec dm) { vec_sync_to_device(dm); }
+
+void get_dm_element(Vec dm, PetscInt row, PetscInt col, PetscScalar *val) {
+  const int64_t loc = dm_side(dm) * col + row;
+  if (loc < 0 || loc >= dm->n) { *val = PetscScalar(0.0, 0.0); return; }
+  if (dm->host_pending) { *val = PetscScalar(dm->h[loc].real(), dm->h[loc].imag()); return; }
+  double2 x;
+  QCUDA(cudaMemcpy(&x, dm->d + loc, sizeof(double2), cudaMemcpyDeviceToHost));
+  *val = PetscScalar(x.x, x.y);
+}
+
+int get_num_populations(void) {
+  qsystem qs = legacy();
+  int np = 0;
+  for (PetscInt i = 0; i < qs->num_subsystems; i++)
+    np += qs->subsystem_list[i]->my_op_type == VEC ? (int)qs->subsystem_list[i]->my_levels : 1;
+  return np;
+}
+
+void get_populations(Vec x, double **populations) {
+  qsystem qs = legacy();
+  vec_sync_to_device(x);
+  const int64_t D = qs->total_levels;
+  const bool dm = qs->dm_equations != 0;
+  if (x->n != (dm ? D * D : D)) { fail(0, "ERROR! get_populations: the vector does not hold the full legacy system\n"); return; }
+  // diagonal of rho (stride D + 1) or the wavefunction, one strided copy
+  std::vector<cplx> dg(D);
+  QCUDA(cudaMemcpy2D(dg.data(), sizeof(double2), x->d, dm ? (D + 1) * sizeof(double2) : sizeof(double2),
+                     sizeof(double2), D, cudaMemcpyDeviceToHost));
+  double *pop = *populations;
+  int np = 0;
+  std::vector<int> first(qs->num_subsystems);
+  for (PetscInt j = 0; j < qs->num_subsystems; j++) {
+    first[j] = np;
+    np += qs->subsystem_list[j]->my_op_type == VEC ? (int)qs->subsystem_list[j]->my_levels : 1;
+  }
+  for (int k = 0; k < np; k++) pop[k] = 0.0;
+  for (int64_t i = 0; i < D; i++) {
+    const double w = dm ? dg[i].real() : std::norm(dg[i]);  // Schroedinger form: |psi_i|^2
+    for (PetscInt j = 0; j < qs->num_subsystems; j++) {
+      op_handle s = qs->subsystem_list[j];
+      const int64_t n_after = D / (s->my_levels * s->n_before);
+      const int64_t cur = (i / n_after) % s->my_levels;
+      if (s->my_op_type == VEC) pop[first[j] + cur] += w;
+      else pop[first[j]] += w * (double)cur;
+    }
+  }
+}
+
 }  // extern "C"
 
 // ------------------------------------------- non-variadic gate entry points
@@ -1202,7 +1319,10 @@ extern "C" int quac_set_deflation_refresh(int mode) {
 }
 
 extern "C" int quac_set_hermitian_mode(int mode) {
-  if (mode != 0 && mode != 1) { fail(0, "ERROR! Hermitian mode must be 0 (off) or 1 (automatic)\n"); return 1; }
+  if (mode < 0 || mode > 2) {
+    fail(0, "ERROR! Hermitian mode must be 0 (off), 1 (automatic in time_step_sys) or 2 (also single L.x)\n");
+    return 1;
+  }
   options().herm_mode = mode;
   return 0;
 }

@@ -125,11 +125,20 @@ struct PassParams {
   int nspill;            // cross-group terms handled with global loads (last pass)
   int ncanon;            // nonzero: canonical single-bit coefficients below are used
   int herm_tiles;        // last pass only: work items are the blocks I <= J, mirrored
+  // first pass of a two-pass Hermitian run: work items are the tile pairs
+  // (a, b), a <= b, of the fixed low bits; tile (b, a) is the conjugate
+  // transpose of tile (a, b), so one load serves both and the pass writes
+  // the running sum of both where the last pass reads it (row >> 6 <= col >> 6)
+  int pair_tiles;
   long long ntiles;
   const double2 *dr, *dc, *gtab;
   const double2 *accin;  // running sum from earlier passes (nullptr: start from zero)
   double2 *accout;       // running sum for later passes
   int *errflag;
+  // dynamic tile queue of the TMA kernels: CTAs claim work items from
+  // *claim; the last CTA to finish (counted in *done) resets both to zero
+  unsigned long long *claim;
+  unsigned *done;
   // TMA view of the tile (used when tma != 0): dims 1..4 of the 5-D tensor
   // map start at flat index bit tstart[d] with tlen[d] bits; tfree[d] marks
   // the dims the box covers fully (their coordinate is 0)
@@ -157,6 +166,8 @@ struct DeviceProgram {
   std::vector<PassParams> passes;  // non-empty: multi-pass qubit kernel
   double2 *scratch = nullptr;      // D^2 running sum for the passes
   int *errflag = nullptr;          // device word set by kernels whose waits time out
+  unsigned *tile_done = nullptr;   // tile-queue words of the pass kernels (same 16-byte block)
+  unsigned long long *tile_claim = nullptr;
   QubitProg qdev{};
   std::vector<QTerm> qterms;  // nL | nR | nJ | nJx in that order
   std::vector<void *> allocations;
@@ -184,6 +195,13 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
                          bool f32 = false);
 // Reads and clears the program's device error word; reports through fail().
 bool check_program_error(DeviceProgram &P, cudaStream_t s);
+// Loads every kernel that launch_lrho_any may run for this program (both
+// contraction precisions) into the current device's context, so that a
+// first launch does not load code (lazy module loading allocates device
+// memory when a kernel is first used).
+void preload_lrho_kernels(const DeviceProgram &P);
+void preload_generic_lrho_kernels();
+void preload_single_pass_qubit_kernels();
 void zero_epi(Epi &e);
 // Raises a kernel's dynamic shared-memory limit on the current device to at
 // least `bytes` (once per kernel, device and size; thread safe).
@@ -196,6 +214,8 @@ double hermitian_asymmetry(const double2 *x, int64_t D, cudaStream_t s);
 void launch_gemm_tf32(const float *A, const float *B, float *C, const float *bias, int M, int N, int K, int act,
                       int *err, cudaStream_t s);
 // lincomb.cu
+void launch_caxpy(double2 *y, const double2 *x, cplx a, int64_t n, cudaStream_t s);
+void launch_epilogue(const double2 *K, const Epi &e, int64_t n, cudaStream_t s);
 void launch_lincomb(double2 *out, const double2 *base, int nin, const double2 *const *in,
                     const double *coef, int64_t n, cudaStream_t s);
 void launch_lincomb_norm(const double2 *base, const double2 *ref, int nin, const double2 *const *in,

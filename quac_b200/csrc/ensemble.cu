@@ -680,6 +680,11 @@ int quac_ensemble_create(quac_ensemble *out, int64_t n, const qsystem *systems) 
   long long yoff = 0, poff = 0;
   for (int64_t i = 0; i < n; i++) {
     HostProg hp;
+    if (!systems[i]->impl->td.empty()) {
+      fail(0, "ERROR! ensemble instance %ld has time-dependent terms (not supported in ensembles)\n", (long)i);
+      delete E;
+      return 1;
+    }
     if (!compile_host(systems[i], 0, hp)) { delete E; return 1; }
     const int D = hp.D;
     if (hp.ncols != D || (long long)D * D > (1 << 24)) {

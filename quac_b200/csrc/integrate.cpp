@@ -31,6 +31,95 @@ void apply_gate_superop(qsystem qs, const struct quantum_gate_struct &g, Vec v, 
                         cudaStream_t s);
 void apply_gate_inplace(qvec q, const struct quantum_gate_struct &g, cudaStream_t s);
 
+cplx TdTerm::scale(double t) const {
+  cplx v;
+  if (f) {
+    const PetscScalar r = f(t, ctx);
+    v = cplx(PetscRealPart(r), PetscImaginaryPart(r));
+  } else {
+    double re = 0.0, im = 0.0;
+    g(t, ctx, &re, &im);
+    v = cplx(re, im);
+  }
+  return term.a * v;
+}
+
+void release_td_programs(qsystem qs) {
+  for (TdTerm &td : qs->impl->td) {
+    if (td.prog) {
+      td.prog->release();
+      delete td.prog;
+      td.prog = nullptr;
+    }
+    td.prog_mode = -1;
+  }
+  if (qs->impl->td_acc) cudaFree(qs->impl->td_acc);
+  qs->impl->td_acc = nullptr;
+  qs->impl->td_acc_n = 0;
+}
+
+namespace {
+
+// Each time-dependent term compiled on its own with coefficient 1
+// (construct_matrix, qsystem.c:642-651), in the system's current mode
+void ensure_td_programs(qsystem qs) {
+  const int mode = qs->dm_equations ? 0 : 1;
+  for (TdTerm &td : qs->impl->td) {
+    if (td.prog && td.prog_mode == mode) continue;
+    if (td.prog) {
+      td.prog->release();
+      delete td.prog;
+      td.prog = nullptr;
+    }
+    std::vector<Term> saved;
+    saved.swap(qs->impl->terms);
+    Term one = td.term;
+    one.a = cplx(1.0, 0.0);
+    qs->impl->terms.push_back(one);
+    td.prog = compile_terms(qs, mode);
+    qs->impl->terms.swap(saved);
+    td.prog_mode = mode;
+    if (!td.prog) return;
+  }
+}
+
+}  // namespace
+
+void apply_L(qsystem qs, double t, const double2 *x, const Epi &e, cudaStream_t s) {
+  qsystem_impl &I = *qs->impl;
+  if (I.td.empty()) {
+    launch_lrho_any(*I.prog, x, e, s);
+    return;
+  }
+  // Y = A X + sum_k a_k f_k(t) A_k X (qsystem.c:1300-1330), then the
+  // stage epilogue on Y
+  ensure_td_programs(qs);
+  if (has_error()) return;
+  const DeviceProgram &P = *I.prog;
+  const int64_t n = (int64_t)P.dev.D * P.dev.ncols;
+  if (I.td_acc_n != n) {
+    if (I.td_acc) QCUDA(cudaFree(I.td_acc));
+    I.td_acc = nullptr;
+    QCUDA(cudaMalloc(&I.td_acc, 2 * (size_t)n * sizeof(double2)));
+    I.td_acc_n = n;
+  }
+  double2 *K = I.td_acc, *T = I.td_acc + n;
+  Epi e0;
+  zero_epi(e0);
+  e0.kout = K;
+  launch_lrho_any(P, x, e0, s);
+  for (const TdTerm &td : I.td) {
+    const cplx sc = td.scale(t);
+    if (std::abs(sc) <= 1e-10) continue;  // min_time_dep, qsystem.c:34, 1320
+    Epi ek;
+    zero_epi(ek);
+    ek.kout = T;
+    launch_lrho_any(*td.prog, x, ek, s);
+    launch_caxpy(K, T, sc, n, s);
+  }
+  launch_epilogue(K, e, n, s);
+}
+
 namespace {
 
 struct Event {
@@ -68,7 +157,8 @@ struct Stepper {
   double atol, rtol;
   int herm;  // Hermitian mode of the multi-pass kernel (see Epi::herm)
 
-  void stage(const double2 *X, std::initializer_list<std::tuple<double2 *, const double2 *, double>> upd,
+  void stage(double ts, const double2 *X,
+             std::initializer_list<std::tuple<double2 *, const double2 *, double>> upd,
              double *nsum = nullptr, int err_upd = 0, const double2 *ny = nullptr,
              const double2 *nyn = nullptr) {
     Epi e;
@@ -88,7 +178,7 @@ struct Stepper {
     e.atol = atol;
     e.rtol = rtol;
     e.herm = herm;
-    launch_lrho_any(*P, X, e, s);
+    apply_L(qs, ts, X, e, s);
   }
 };
 
@@ -123,8 +213,9 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
   // the initial state is Hermitian to rounding; every stage then keeps the
   // state exactly Hermitian (conjugate-transposed blocks are written, not
   // computed)
+  const bool td = !qs->impl->td.empty();
   int herm = 0;
-  if (o.herm_mode && PP.herm_ok && PP.has_qubit && !PP.passes.empty() && P.ncols == P.D && events.empty())
+  if (o.herm_mode && !td && PP.herm_ok && PP.has_qubit && !PP.passes.empty() && P.ncols == P.D && events.empty())
     herm = hermitian_asymmetry(v->d, P.D, s) <= 1e-13 ? 1 : 0;
   Stepper st{qs, &PP, s, n, o.atol, o.rtol, herm};
   size_t next_ev = 0;
@@ -169,7 +260,7 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
         zero_epi(e);
         e.kout = K[st_i];
         e.herm = herm;
-        launch_lrho_any(PP, X, e, s);
+        apply_L(qs, t + kDP_C[st_i] * h_try, X, e, s);
       }
       // xs now holds the fifth-order solution (input of stage 7)
       double c[7];
@@ -189,34 +280,34 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
         if (accepted) std::swap(v->d, W.bufs[7]);
         if (!accepted) { h = h_next; continue; }
       }
-    } else if (fixed && rk4 && !o.rk4_classic) {
+    } else if (fixed && rk4 && !o.rk4_classic && !td) {
       // For a time-independent linear right-hand side the classical RK4 step
       // equals the degree-4 Taylor polynomial of exp(hL); evaluated by
       // Horner's rule each stage reads one vector besides its input:
       //   v <- y + (h/4) L y;  v <- y + (h/3) L v;  v <- y + (h/2) L v;  y <- y + h L v
       double2 *va = W.bufs[0], *vb = W.bufs[1];
-      st.stage(y, {{va, y, h_try / 4.0}});
-      st.stage(va, {{vb, y, h_try / 3.0}});
-      st.stage(vb, {{va, y, h_try / 2.0}});
-      st.stage(va, {{y, y, h_try}});
+      st.stage(t, y, {{va, y, h_try / 4.0}});
+      st.stage(t, va, {{vb, y, h_try / 3.0}});
+      st.stage(t, vb, {{va, y, h_try / 2.0}});
+      st.stage(t, va, {{y, y, h_try}});
     } else if (fixed && rk4) {
       double2 *acc = W.bufs[0], *xa = W.bufs[1], *xb = W.bufs[2];
-      st.stage(y, {{acc, y, h_try / 6.0}, {xa, y, h_try / 2.0}});
-      st.stage(xa, {{acc, acc, h_try / 3.0}, {xb, y, h_try / 2.0}});
-      st.stage(xb, {{acc, acc, h_try / 3.0}, {xa, y, h_try}});
-      st.stage(xa, {{y, acc, h_try / 6.0}});
+      st.stage(t, y, {{acc, y, h_try / 6.0}, {xa, y, h_try / 2.0}});
+      st.stage(t + 0.5 * h_try, xa, {{acc, acc, h_try / 3.0}, {xb, y, h_try / 2.0}});
+      st.stage(t + 0.5 * h_try, xb, {{acc, acc, h_try / 3.0}, {xa, y, h_try}});
+      st.stage(t + h_try, xa, {{y, acc, h_try / 6.0}});
     } else {
       // Bogacki-Shampine 3(2): c = (0, 1/2, 3/4, 1), b = (2/9, 1/3, 4/9, 0),
       // bhat = (7/24, 1/4, 1/3, 1/8); error = h * sum (b - bhat)_i k_i.
       double2 *x1 = W.bufs[0], *x2 = W.bufs[1], *yn = W.bufs[2], *er = W.bufs[3];
-      st.stage(y, {{x1, y, 0.5 * h_try}, {yn, y, 2.0 / 9.0 * h_try}, {er, nullptr, (2.0 / 9.0 - 7.0 / 24.0) * h_try}});
-      st.stage(x1, {{x2, y, 0.75 * h_try}, {yn, yn, h_try / 3.0}, {er, er, (1.0 / 3.0 - 0.25) * h_try}});
-      st.stage(x2, {{yn, yn, 4.0 / 9.0 * h_try}, {er, er, (4.0 / 9.0 - 1.0 / 3.0) * h_try}});
+      st.stage(t, y, {{x1, y, 0.5 * h_try}, {yn, y, 2.0 / 9.0 * h_try}, {er, nullptr, (2.0 / 9.0 - 7.0 / 24.0) * h_try}});
+      st.stage(t + 0.5 * h_try, x1, {{x2, y, 0.75 * h_try}, {yn, yn, h_try / 3.0}, {er, er, (1.0 / 3.0 - 0.25) * h_try}});
+      st.stage(t + 0.75 * h_try, x2, {{yn, yn, 4.0 / 9.0 * h_try}, {er, er, (4.0 / 9.0 - 1.0 / 3.0) * h_try}});
       if (fixed) {
         std::swap(v->d, W.bufs[2]);
       } else {
         QCUDA(cudaMemsetAsync(W.dsum, 0, sizeof(double), s));
-        st.stage(yn, {{er, er, -0.125 * h_try}}, W.dsum, 0, y, yn);
+        st.stage(t + h_try, yn, {{er, er, -0.125 * h_try}}, W.dsum, 0, y, yn);
         QCUDA(cudaMemcpyAsync(W.hsum, W.dsum, sizeof(double), cudaMemcpyDeviceToHost, s));
         QCUDA(cudaStreamSynchronize(s));
         const double err = std::sqrt(W.hsum[0] / (double)n);
@@ -265,6 +356,15 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
   return has_error() ? 1 : 0;
 }
 
+// Hermitian mode 2 for a single L.x: the program supports it and x is
+// Hermitian to 1e-13 (relative Frobenius asymmetry)
+int apply_herm(qsystem qs, const double2 *x, cudaStream_t s) {
+  const DeviceProgram &PP = *qs->impl->prog;
+  if (options().herm_mode != 2 || !qs->impl->td.empty() || !PP.herm_ok || !PP.has_qubit || PP.passes.empty() || PP.dev.ncols != PP.dev.D)
+    return 0;
+  return hermitian_asymmetry(x, PP.dev.D, s) <= 1e-13 ? 1 : 0;
+}
+
 }  // namespace quac
 
 using namespace quac;
@@ -295,7 +395,8 @@ int quac_lrho_apply_device(qsystem qs, const void *x_dev, void *y_dev) {
   zero_epi(e);
   e.kout = (double2 *)y_dev;
   cudaStream_t s = stream_of(qs);
-  launch_lrho_any(*qs->impl->prog, (const double2 *)x_dev, e, s);
+  e.herm = apply_herm(qs, (const double2 *)x_dev, s);
+  apply_L(qs, qs->current_time, (const double2 *)x_dev, e, s);
   QCUDA(cudaStreamSynchronize(s));
   check_program_error(*qs->impl->prog, s);
   return has_error() ? 1 : 0;
@@ -309,10 +410,12 @@ int quac_lrho_apply_host(qsystem qs, const PetscScalar *x_host, PetscScalar *y_h
   cudaStream_t s = stream_of(qs);
   QCUDA(cudaMemcpyAsync(W.bufs[0], x_host, n * sizeof(double2), cudaMemcpyHostToDevice, s));
   ensure_program(qs);
+  if (has_error()) return 1;
   Epi e;
   zero_epi(e);
   e.kout = W.bufs[1];
-  launch_lrho_any(*qs->impl->prog, W.bufs[0], e, s);
+  e.herm = apply_herm(qs, W.bufs[0], s);
+  apply_L(qs, qs->current_time, W.bufs[0], e, s);
   QCUDA(cudaMemcpyAsync(y_host, W.bufs[1], n * sizeof(double2), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));
   check_program_error(*qs->impl->prog, s);

@@ -103,7 +103,65 @@ __global__ void k_herm_asym(const double2 *__restrict__ x, int64_t D, double *su
   }
 }
 
+// y[i] += a * x[i] (complex a): one time-dependent term's contribution
+__global__ void k_caxpy(double2 *__restrict__ y, const double2 *__restrict__ x, double2 a, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    const double2 v = x[i];
+    double2 w = y[i];
+    w.x = fma(a.x, v.x, fma(-a.y, v.y, w.x));
+    w.y = fma(a.x, v.y, fma(a.y, v.x, w.y));
+    y[i] = w;
+  }
+}
+
+// The stage epilogue of the fused L.x kernels (Epi) applied to a given
+// K = L x: kout, up to three updates base_u + coef_u K and the error norm
+__global__ void k_epilogue(const double2 *__restrict__ K, const Epi E, int64_t n) {
+  __shared__ double red[NT / 32];
+  double loc = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    const double2 k = K[i];
+    if (E.kout) E.kout[i] = k;
+    double2 u[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+    for (int j = 0; j < E.nupd; j++) {
+      const double2 b = E.base[j] ? E.base[j][i] : make_double2(0.0, 0.0);
+      u[j] = make_double2(fma(E.coef[j], k.x, b.x), fma(E.coef[j], k.y, b.y));
+      E.out[j][i] = u[j];
+    }
+    if (E.nsum) {
+      const double2 ev = u[E.err_upd];
+      const double2 y = E.ny[i];
+      const double2 yn = E.yn_upd >= 0 ? u[E.yn_upd] : E.nyn[i];
+      const double q = sqrt(ev.x * ev.x + ev.y * ev.y) /
+                       (E.atol + E.rtol * fmax(sqrt(y.x * y.x + y.y * y.y), sqrt(yn.x * yn.x + yn.y * yn.y)));
+      loc += q * q;
+    }
+  }
+  if (E.nsum) {
+    for (int o = 16; o > 0; o >>= 1) loc += __shfl_down_sync(0xffffffffu, loc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = loc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; w++) t += red[w];
+      atomicAdd(E.nsum, t);
+    }
+  }
+}
+
 }  // namespace
+
+void launch_caxpy(double2 *y, const double2 *x, cplx a, int64_t n, cudaStream_t s) {
+  k_caxpy<<<grid_of(n), NT, 0, s>>>(y, x, make_double2(a.real(), a.imag()), n);
+  count_launch();
+  QCUDA(cudaGetLastError());
+}
+
+void launch_epilogue(const double2 *K, const Epi &e, int64_t n, cudaStream_t s) {
+  k_epilogue<<<grid_of(n), NT, 0, s>>>(K, e, n);
+  count_launch();
+  QCUDA(cudaGetLastError());
+}
 
 void launch_lincomb(double2 *out, const double2 *base, int nin, const double2 *const *in,
                     const double *coef, int64_t n, cudaStream_t s) {

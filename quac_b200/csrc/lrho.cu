@@ -282,6 +282,15 @@ void ensure_smem(const void *func, size_t bytes) {
   if (!has_error()) have = bytes;
 }
 
+void preload_generic_lrho_kernels() {
+  cudaFuncAttributes fa;
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho_split<8>));
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho<1>));
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho<2>));
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho<4>));
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho<8>));
+}
+
 void zero_epi(Epi &e) {
   memset(&e, 0, sizeof(Epi));
   e.err_upd = 0;

@@ -5,15 +5,19 @@
 // applied to rows and columns alike.  Pass p owns 64 x 64 tiles whose free
 // bits are group p for rows and columns; every term whose flip mask lies in
 // group p (left: row flips, right: column flips, jumps: both) finds its
-// partners inside the tile.  Pass 0 also applies the diagonal.  Passes
-// accumulate into a scratch vector; the last one runs the fused stage
-// epilogue.  A CTA is persistent (one per SM) and streams tiles through two
-// shared-memory buffers filled by cp.async, so the next tile's loads overlap
-// the current tile's arithmetic.
+// partners inside the tile.  The high groups run first and accumulate into a
+// running-sum vector; the pass over group 0 (contiguous rows) also applies
+// the diagonal and runs the fused stage epilogue.  CTAs are persistent (one
+// per SM), claim work items from a queue in global memory and stream tiles
+// through three shared-memory stages filled by TMA, so the next tiles' loads
+// overlap the current tile's arithmetic.
 //
-// Consecutive work items differ in the lowest fixed row bit, so in passes
-// whose tiles have single-element rows the two halves of every 32-byte
-// sector are requested by neighbouring CTAs at the same time.
+// Hermitian mode (x Hermitian, L Hermiticity-preserving): the last pass
+// computes only the 64 x 64 blocks I <= J of the bits above group 0 and
+// writes each off-diagonal block's conjugate transpose as well.  In a
+// two-pass program the first pass then works on tile pairs: tile (b, a) of
+// its fixed low bits is the conjugate transpose of tile (a, b), so one load
+// serves both, halving that pass's reads of x.
 #include <algorithm>
 #include <array>
 #include <cstring>
@@ -97,19 +101,31 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// triangular work index t = b (b + 1) / 2 + a  ->  (a, b), a <= b
+__device__ __forceinline__ void tri_index(long long t, unsigned &a, unsigned &b) {
+  long long J = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((J + 1) * (J + 2) / 2 <= t) J++;
+  while (J * (J + 1) / 2 > t) J--;
+  a = (unsigned)(t - J * (J + 1) / 2);
+  b = (unsigned)J;
+}
+
 // fixed (non-tile) bits of a work item: rows then columns
-__device__ __forceinline__ void tile_origin(long long t, int n, int lo, unsigned &rfix, unsigned &cfix,
-                                            int herm = 0) {
-  if (herm) {
-    // work item t = J (J + 1) / 2 + I over the blocks I <= J of the high bits (lo == 0)
-    long long J = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((J + 1) * (J + 2) / 2 <= t) J++;
-    while (J * (J + 1) / 2 > t) J--;
-    const long long I = t - J * (J + 1) / 2;
-    rfix = (unsigned)(I << 6);
-    cfix = (unsigned)(J << 6);
+__device__ __forceinline__ void tile_origin(const PassParams &P, long long t, unsigned &rfix, unsigned &cfix) {
+  if (P.herm_tiles) {
+    // blocks I <= J of the bits above the low group (lo == 0)
+    unsigned I, J;
+    tri_index(t, I, J);
+    rfix = I << 6;
+    cfix = J << 6;
     return;
   }
+  if (P.pair_tiles) {
+    // tile pairs a <= b of the fixed low bits [0, lo) (lo + 6 == n)
+    tri_index(t, rfix, cfix);
+    return;
+  }
+  const int n = P.n, lo = P.lo;
   const int hi = lo + 6;
   const unsigned lowmask = (1u << lo) - 1u;
   const int nhigh = n - hi;
@@ -125,13 +141,13 @@ __device__ __forceinline__ void tile_origin(long long t, int n, int lo, unsigned
 }
 
 __device__ __forceinline__ void load_tile(double2 *buf, const double2 *__restrict__ X, long long t,
-                                          int n, int lo, int herm = 0) {
+                                          const PassParams &P) {
   unsigned rfix, cfix;
-  tile_origin(t, n, lo, rfix, cfix, herm);
-  const size_t D = (size_t)1 << n;
+  tile_origin(P, t, rfix, cfix);
+  const size_t D = (size_t)1 << P.n;
   for (int e = threadIdx.x; e < NEL; e += blockDim.x) {
     const unsigned cl = e >> 6, rl = e & 63;
-    const size_t r = rfix | (rl << lo), c = cfix | (cl << lo);
+    const size_t r = rfix | (rl << P.lo), c = cfix | (cl << P.lo);
     cp_async16(buf + e, X + c * D + r);
   }
 }
@@ -140,7 +156,7 @@ __device__ __forceinline__ void load_tile(double2 *buf, const double2 *__restric
 __device__ __forceinline__ void tma_tile(const PassParams &P, const CUtensorMap *map, double2 *buf,
                                          uint64_t *bar, long long t) {
   unsigned rfix, cfix;
-  tile_origin(t, P.n, P.lo, rfix, cfix, P.herm_tiles);
+  tile_origin(P, t, rfix, cfix);
   const unsigned long long F = (unsigned long long)rfix | ((unsigned long long)cfix << P.n);
   int c[5] = {0, 0, 0, 0, 0};
 #pragma unroll
@@ -150,72 +166,125 @@ __device__ __forceinline__ void tma_tile(const PassParams &P, const CUtensorMap 
   tma_load_5d(buf, map, bar, c[0], c[1], c[2], c[3], c[4]);
 }
 
-// NTHR threads per CTA; each thread owns rows lane, lane+32 and MC columns
-// w, w + NW, ... (NW = NTHR / 32 warps).  CANON (real mode only) is a
-// compile-time mask of the canonical single-bit kinds present: 1 = left X,
-// 2 = right X, 4 = lowering jump, 8 = raising jump; CANON < 0 means the
-// kinds are decided at run time.
-template <bool REAL, bool TMA, int NTHR, int CANON, bool F32>
-__global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassParams P,
-                                                   const __grid_constant__ CUtensorMap tmap,
-                                                   const double2 *__restrict__ X, const Epi E) {
-  constexpr int PT = NTHR;
-  constexpr int NW = NTHR / 32;
-  constexpr int MC = 64 / NW;
-  constexpr int NST = TMA ? 3 : 2;   // pipeline stages
+// waits for phase `parity` of bar for at most `limit_ns`; false on time-out
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, unsigned long long limit_ns) {
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
+}
+
+// stage value base_u + coef_u K of the epilogue (base of update 0 from registers)
+__device__ __forceinline__ double2 stage_value(const Epi &E, int u, size_t idx, double2 Kv, double2 b0) {
+  double2 b = u == 0 ? b0 : (E.base[u] ? E.base[u][idx] : make_double2(0.0, 0.0));
+  return make_double2(fma(E.coef[u], Kv.x, b.x), fma(E.coef[u], Kv.y, b.y));
+}
+
+constexpr int QT = 512;          // threads of the pass kernel
+constexpr int QNW = QT / 32;     // warps
+constexpr int QMC = 64 / QNW;    // tile columns per thread
+
+// One pass over 64 x 64 tiles.  Thread (lane, w) owns tile rows lane,
+// lane + 32 and columns w, w + 16, w + 32, w + 48; its eight values sit in
+// registers, so flips of row bit 5 and of column bits 4 and 5 need no
+// shared-memory read.  CANON (real mode only) is a compile-time mask of the
+// canonical single-bit kinds present: 1 = left X, 2 = right X, 4 = lowering
+// jump, 8 = raising jump; CANON < 0 means the kinds are decided at run
+// time.  With TMA the CTAs are persistent, claim work items from a queue
+// when they issue the load (two items ahead, three stages), and prefetch
+// the running sum and the first stage base into registers before waiting
+// for the tile.
+template <bool REAL, bool TMA, int CANON, bool F32>
+__global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassParams P,
+                                                 const __grid_constant__ CUtensorMap tmap,
+                                                 const __grid_constant__ CUtensorMap bmap,
+                                                 const double2 *__restrict__ X, const Epi E) {
+  constexpr int NST = TMA ? 3 : 2;   // shared-memory buffers of NEL values
   // complex128 contraction, or (F32) complex64 contraction of tiles
   // converted in shared memory, accumulated in complex64
   using V2 = typename std::conditional<F32, float2, double2>::type;
   using S = typename std::conditional<F32, float, double>::type;
   extern __shared__ __align__(128) double2 sm[];
   double2 *gts = sm + NST * NEL;     // ngroups * 64, layout [g][col bits][row bits]
-  __shared__ double red[PT / 32];
-  __shared__ __align__(8) uint64_t bars[3];
+  __shared__ double red[QNW];
+  __shared__ __align__(8) uint64_t bars[4];
+  __shared__ long long tids[3];
+  // last pass with TMA: the first stage base of each tile comes by TMA into
+  // the third buffer, and the tiles of x use two stages
+  const bool bt = TMA && P.last && E.nupd > 0 && E.base[0] != nullptr;
+  const int nst = TMA ? (bt ? 2 : 3) : 2;
+  const double2 *bbuf = sm + 2 * NEL;
   const int n = P.n, lo = P.lo;
   const size_t D = (size_t)1 << n;
   if (P.diag)
-    for (int i = threadIdx.x; i < P.ngroups * 64; i += PT) {
+    for (int i = threadIdx.x; i < P.ngroups * 64; i += QT) {
       const int g = i >> 6, rb = (i >> 3) & 7, cb = i & 7;  // source layout [g][rb][cb]
       gts[(g << 6) | (cb << 3) | rb] = P.gtab[i];
     }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double nloc = 0.0;
+  bool timed_out = false;
+  int it = 0;
   if (TMA) {
     if (threadIdx.x == 0) {
-      for (int q = 0; q < 3; q++) mbar_init(&bars[q], 1);
+      for (int q = 0; q < 4; q++) mbar_init(&bars[q], 1);
       asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int q = 0; q < 2; q++) {
-        const long long tq = blockIdx.x + (long long)q * gridDim.x;
+      for (int q = 0; q < nst - 1; q++) {
+        const long long tq = (long long)atomicAdd(P.claim, 1ull);
+        tids[q] = tq;
         if (tq < P.ntiles) tma_tile(P, &tmap, sm + q * NEL, &bars[q], tq);
       }
     }
   } else {
-    if (blockIdx.x < P.ntiles) load_tile(sm, X, blockIdx.x, n, lo, P.herm_tiles);
+    if (blockIdx.x < P.ntiles) load_tile(sm, X, blockIdx.x, P);
     cp_commit();
   }
-  long long t = blockIdx.x;
-  for (int it = 0; t < P.ntiles; it++, t += gridDim.x) {
-    double2 *cur = sm + (it % NST) * NEL;
+  __syncthreads();
+  long long t_static = blockIdx.x;
+  for (;; it++) {
+    const long long t = TMA ? tids[it % nst] : t_static;
+    if (t >= P.ntiles) break;
+    double2 *cur = sm + (it % nst) * NEL;
+    if (TMA && threadIdx.x == 0) {
+      const int q2 = (it + nst - 1) % nst;
+      const long long t2 = (long long)atomicAdd(P.claim, 1ull);
+      tids[q2] = t2;
+      if (t2 < P.ntiles) tma_tile(P, &tmap, sm + q2 * NEL, &bars[q2], t2);
+      if (bt) tma_tile(P, &bmap, sm + 2 * NEL, &bars[3], t);
+    }
+    unsigned rfix, cfix;
+    tile_origin(P, t, rfix, cfix);
+    // an off-diagonal block also stands for its conjugate transpose
+    const bool mirror = P.herm_tiles && rfix != cfix;
+    unsigned rl[2] = {(unsigned)lane, (unsigned)lane + 32u};
+    unsigned cl[QMC];
+#pragma unroll
+    for (int m = 0; m < QMC; m++) cl[m] = (unsigned)(w + QNW * m);
+    unsigned r[2], c[QMC];
+#pragma unroll
+    for (int i = 0; i < 2; i++) r[i] = rfix | (rl[i] << lo);
+#pragma unroll
+    for (int m = 0; m < QMC; m++) c[m] = cfix | (cl[m] << lo);
+    // loads that do not depend on the tile go out before the wait
+    V2 acc[2][QMC];
+    if (P.accin) {
+      const V2 *ain = reinterpret_cast<const V2 *>(P.accin);
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int m = 0; m < QMC; m++) acc[i][m] = ain[(size_t)c[m] * D + r[i]];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int m = 0; m < QMC; m++) acc[i][m] = to_v2<V2>(make_double2(0.0, 0.0));
+    }
     if (TMA) {
-      const long long t2 = t + 2ll * gridDim.x;
-      if (threadIdx.x == 0 && t2 < P.ntiles)
-        tma_tile(P, &tmap, sm + ((it + 2) % 3) * NEL, &bars[(it + 2) % 3], t2);
-      const unsigned parity = (unsigned)((it / 3) & 1);
-      const unsigned long long t0 = global_ns();
-      bool timed_out = false;
-      while (!mbar_try_wait(&bars[it % 3], parity)) {
-        if (global_ns() - t0 > 2000000000ull) { timed_out = true; break; }
-      }
-      if (__syncthreads_or(timed_out)) {
-        if (threadIdx.x == 0 && P.errflag) atomicExch(P.errflag, 1);
-        return;
-      }
+      const bool ok = mbar_wait_bounded(&bars[it % nst], (unsigned)((it / nst) & 1), 2000000000ull);
+      if (__syncthreads_or(!ok)) { timed_out = true; break; }
     } else {
       const long long tn = t + gridDim.x;
-      if (tn < P.ntiles) load_tile(sm + ((it + 1) & 1) * NEL, X, tn, n, lo, P.herm_tiles);
+      if (tn < P.ntiles) load_tile(sm + ((it + 1) & 1) * NEL, X, tn, P);
       cp_commit();
       cp_wait<1>();
       __syncthreads();
@@ -224,42 +293,21 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
     if (F32) {
       // in place: every thread reads its complex128 elements before any
       // complex64 value is written over them
-      double2 tmp[NEL / PT];
+      double2 tmp[NEL / QT];
 #pragma unroll
-      for (int k2 = 0; k2 < NEL / PT; k2++) tmp[k2] = cur[threadIdx.x + k2 * PT];
+      for (int k2 = 0; k2 < NEL / QT; k2++) tmp[k2] = cur[threadIdx.x + k2 * QT];
       __syncthreads();
       float2 *c32 = reinterpret_cast<float2 *>(cur);
 #pragma unroll
-      for (int k2 = 0; k2 < NEL / PT; k2++)
-        c32[threadIdx.x + k2 * PT] = make_float2((float)tmp[k2].x, (float)tmp[k2].y);
+      for (int k2 = 0; k2 < NEL / QT; k2++)
+        c32[threadIdx.x + k2 * QT] = make_float2((float)tmp[k2].x, (float)tmp[k2].y);
       __syncthreads();
     }
-    unsigned rfix, cfix;
-    tile_origin(t, n, lo, rfix, cfix, P.herm_tiles);
-    // an off-diagonal block also stands for its conjugate transpose
-    const bool mirror = P.herm_tiles && rfix != cfix;
-    unsigned rl[2] = {(unsigned)lane, (unsigned)lane + 32u};
-    unsigned cl[MC];
+    V2 xo[2][QMC];  // own values
 #pragma unroll
-    for (int m = 0; m < MC; m++) cl[m] = (unsigned)(w + NW * m);
-    unsigned r[2], c[MC];
+    for (int i = 0; i < 2; i++)
 #pragma unroll
-    for (int i = 0; i < 2; i++) r[i] = rfix | (rl[i] << lo);
-#pragma unroll
-    for (int m = 0; m < MC; m++) c[m] = cfix | (cl[m] << lo);
-    V2 acc[2][MC];
-    if (P.accin) {
-      const V2 *ain = reinterpret_cast<const V2 *>(P.accin);
-#pragma unroll
-      for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int m = 0; m < MC; m++) acc[i][m] = ain[(size_t)c[m] * D + r[i]];
-    } else {
-#pragma unroll
-      for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int m = 0; m < MC; m++) acc[i][m] = to_v2<V2>(make_double2(0.0, 0.0));
-    }
+      for (int m = 0; m < QMC; m++) xo[i][m] = tile[cl[m] * 64 + rl[i]];
     if (P.diag) {
       // groups 0 and 1 vary inside the tile (lo == 0 here); the others are
       // fixed by the tile origin
@@ -275,7 +323,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         dri.x += gconst.x;
         dri.y += gconst.y;
 #pragma unroll
-        for (int m = 0; m < MC; m++) {
+        for (int m = 0; m < QMC; m++) {
           double2 d = __ldg(P.dc + c[m]);
           d.x += dri.x;
           d.y += dri.y;
@@ -287,7 +335,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
             d.x += v1.x;
             d.y += v1.y;
           }
-          cfma2(acc[i][m], to_v2<V2>(d), tile[cl[m] * 64 + rl[i]]);
+          cfma2(acc[i][m], to_v2<V2>(d), xo[i][m]);
         }
       }
     }
@@ -296,7 +344,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
       constexpr bool C_GL = CANON < 0 || (CANON & 4), C_GU = CANON < 0 || (CANON & 8);
       // canonical single-bit terms: partner offsets are compile-time
       // constants; absent kinds are compiled out, zero coefficients are
-      // applied as zeros (no branches between terms)
+      // applied as zeros (no branches between terms).  Partners across row
+      // bit 5 or column bits 4, 5 come from the thread's own registers.
 #pragma unroll
       for (int b = 0; b < 6; b++) {
         const unsigned f = 1u << b;
@@ -305,8 +354,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int m = 0; m < MC; m++) {
-              const V2 p = tile[cl[m] * 64 + (rl[i] ^ f)];
+            for (int m = 0; m < QMC; m++) {
+              const V2 p = b == 5 ? xo[i ^ 1][m] : tile[cl[m] * 64 + (rl[i] ^ f)];
               acc[i][m].x = fma(-hl, p.y, acc[i][m].x);
               acc[i][m].y = fma(hl, p.x, acc[i][m].y);
             }
@@ -316,8 +365,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int m = 0; m < MC; m++) {
-              const V2 p = tile[(cl[m] ^ f) * 64 + rl[i]];
+            for (int m = 0; m < QMC; m++) {
+              const V2 p = b == 5 ? xo[i][m ^ 2] : (b == 4 ? xo[i][m ^ 1] : tile[(cl[m] ^ f) * 64 + rl[i]]);
               acc[i][m].x = fma(-hr, p.y, acc[i][m].x);
               acc[i][m].y = fma(hr, p.x, acc[i][m].y);
             }
@@ -327,10 +376,10 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
 #pragma unroll
           for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int m = 0; m < MC; m++) {
+            for (int m = 0; m < QMC; m++) {
               const bool rb = rl[i] & f, cb = cl[m] & f;
               const S g = (rb != cb) ? (S)0 : (rb ? gu : gl);
-              const V2 p = tile[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
+              const V2 p = b == 5 ? xo[i ^ 1][m ^ 2] : tile[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
               acc[i][m].x = fma(g, p.x, acc[i][m].x);
               acc[i][m].y = fma(g, p.y, acc[i][m].y);
             }
@@ -348,7 +397,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         if (REAL) {
           const S wv = (S)(neg ? -T.coef.y : T.coef.y);
 #pragma unroll
-          for (int m = 0; m < MC; m++) {
+          for (int m = 0; m < QMC; m++) {
             const V2 p = tile[cl[m] * 64 + pr];
             acc[i][m].x = fma(-wv, p.y, acc[i][m].x);
             acc[i][m].y = fma(wv, p.x, acc[i][m].y);
@@ -356,14 +405,14 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         } else {
           const V2 wv = to_v2<V2>(neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef);
 #pragma unroll
-          for (int m = 0; m < MC; m++) cfma2(acc[i][m], wv, tile[cl[m] * 64 + pr]);
+          for (int m = 0; m < QMC; m++) cfma2(acc[i][m], wv, tile[cl[m] * 64 + pr]);
         }
       }
     }
     for (int e = k + P.nR; k < e; k++) {
       const PassTerm T = P.t[k];
 #pragma unroll
-      for (int m = 0; m < MC; m++) {
+      for (int m = 0; m < QMC; m++) {
         if ((c[m] & T.cmask) != T.cval) continue;
         const bool neg = __popc(c[m] & T.smask) & 1;
         const unsigned pc = cl[m] ^ T.fl;
@@ -390,7 +439,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         const int sr = __popc(r[i] & T.smask);
         const unsigned pr = rl[i] ^ T.fl;
 #pragma unroll
-        for (int m = 0; m < MC; m++) {
+        for (int m = 0; m < QMC; m++) {
           if ((c[m] & T.cmask) != T.cval) continue;
           const bool neg = (sr + __popc(c[m] & T.smask)) & 1;
           const V2 p = tile[(cl[m] ^ T.fl) * 64 + pr];
@@ -411,16 +460,16 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         if ((r[i] & T.cmask) != T.cval) continue;
         const int sr = __popc(r[i] & T.smask);
 #pragma unroll
-        for (int m = 0; m < MC; m++) {
+        for (int m = 0; m < QMC; m++) {
           if ((c[m] & T.cmask) != T.cval) continue;
           const bool neg = (sr + __popc(c[m] & T.smask)) & 1;
-          cfma2(acc[i][m], to_v2<V2>(neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef), tile[cl[m] * 64 + rl[i]]);
+          cfma2(acc[i][m], to_v2<V2>(neg ? make_double2(-T.coef.x, -T.coef.y) : T.coef), xo[i][m]);
         }
       }
     }
     // cross-group terms (flip bits in two groups): global loads.  Stored
     // after the pass's own terms with fl holding the full flip mask and the
-    // kind in cval's top bits is not needed: kind order L, R, J.
+    // kind (L, R, J) in its top bits.
     for (int s = 0; s < P.nspill; s++, k++) {
       const PassTerm T = P.t[k];
       const int kind = (int)(T.fl >> 29);
@@ -428,7 +477,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
 #pragma unroll
       for (int i = 0; i < 2; i++) {
 #pragma unroll
-        for (int m = 0; m < MC; m++) {
+        for (int m = 0; m < QMC; m++) {
           const bool okr = (r[i] & T.cmask) == T.cval, okc = (c[m] & T.cmask) == T.cval;
           size_t pidx;
           int sg;
@@ -450,183 +499,133 @@ __global__ void __launch_bounds__(NTHR, 1) k_qpass(const __grid_constant__ PassP
         }
       }
     }
-    // outputs
+    if (bt) {
+      const bool ok = mbar_wait_bounded(&bars[3], (unsigned)(it & 1), 2000000000ull);
+      if (__syncthreads_or(!ok)) { timed_out = true; break; }
+    }
+    // first stage base of element (i, m)
+    auto base0 = [&](int i, int m, size_t idx) -> double2 {
+      if (bt) return bbuf[cl[m] * 64 + rl[i]];
+      return (E.nupd > 0 && E.base[0]) ? E.base[0][idx] : make_double2(0.0, 0.0);
+    };
+    if (!P.last) {
+      // running sum for the later passes
+      V2 *aout = reinterpret_cast<V2 *>(P.accout);
 #pragma unroll
-    for (int i = 0; i < 2; i++) {
+      for (int i = 0; i < 2; i++)
 #pragma unroll
-      for (int m = 0; m < MC; m++) {
-        const size_t idx = (size_t)c[m] * D + r[i];
-        if (!P.last) {
-          reinterpret_cast<V2 *>(P.accout)[idx] = acc[i][m];
-          continue;
+        for (int m = 0; m < QMC; m++) {
+          if (!P.pair_tiles) {
+            aout[(size_t)c[m] * D + r[i]] = acc[i][m];
+            continue;
+          }
+          // tile (a, b) at its own positions, and its conjugate transpose at
+          // the transposed positions (those of tile (b, a)), wherever the
+          // last pass reads the running sum
+          if ((r[i] >> 6) <= (c[m] >> 6)) aout[(size_t)c[m] * D + r[i]] = acc[i][m];
+          if (rfix != cfix && (c[m] >> 6) <= (r[i] >> 6)) {
+            V2 v = acc[i][m];
+            v.y = -v.y;
+            aout[(size_t)r[i] * D + c[m]] = v;
+          }
         }
-        const double2 Kv = make_double2((double)acc[i][m].x, (double)acc[i][m].y);
-        if (E.kout) E.kout[idx] = Kv;
-        double2 u0 = make_double2(0.0, 0.0), u1 = u0, u2 = u0;
-        if (E.nupd > 0) {
-          double2 b = E.base[0] ? E.base[0][idx] : make_double2(0.0, 0.0);
-          u0 = make_double2(fma(E.coef[0], Kv.x, b.x), fma(E.coef[0], Kv.y, b.y));
-          E.out[0][idx] = u0;
-        }
-        if (E.nupd > 1) {
-          double2 b = E.base[1] ? E.base[1][idx] : make_double2(0.0, 0.0);
-          u1 = make_double2(fma(E.coef[1], Kv.x, b.x), fma(E.coef[1], Kv.y, b.y));
-          E.out[1][idx] = u1;
-        }
-        if (E.nupd > 2) {
-          double2 b = E.base[2] ? E.base[2][idx] : make_double2(0.0, 0.0);
-          u2 = make_double2(fma(E.coef[2], Kv.x, b.x), fma(E.coef[2], Kv.y, b.y));
-          E.out[2][idx] = u2;
-        }
-        if (E.nsum) {
-          const double2 ev = E.err_upd == 0 ? u0 : (E.err_upd == 1 ? u1 : u2);
-          const double2 y = E.ny[idx];
-          const double2 yn = E.yn_upd == 0 ? u0 : (E.yn_upd == 1 ? u1 : (E.yn_upd == 2 ? u2 : E.nyn[idx]));
-          const double q = cabs2d(ev) / (E.atol + E.rtol * fmax(cabs2d(y), cabs2d(yn)));
-          nloc += mirror ? 2.0 * q * q : q * q;
+    } else if (!P.herm_tiles) {
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+#pragma unroll
+        for (int m = 0; m < QMC; m++) {
+          const size_t idx = (size_t)c[m] * D + r[i];
+          const double2 Kv = make_double2((double)acc[i][m].x, (double)acc[i][m].y);
+          if (E.kout) E.kout[idx] = Kv;
+          double2 u0 = make_double2(0.0, 0.0), u1 = u0, u2 = u0;
+          const double2 b0 = base0(i, m, idx);
+          if (E.nupd > 0) E.out[0][idx] = u0 = stage_value(E, 0, idx, Kv, b0);
+          if (E.nupd > 1) E.out[1][idx] = u1 = stage_value(E, 1, idx, Kv, b0);
+          if (E.nupd > 2) E.out[2][idx] = u2 = stage_value(E, 2, idx, Kv, b0);
+          if (E.nsum) {
+            const double2 ev = E.err_upd == 0 ? u0 : (E.err_upd == 1 ? u1 : u2);
+            const double2 y = E.ny[idx];
+            const double2 yn = E.yn_upd == 0 ? u0 : (E.yn_upd == 1 ? u1 : (E.yn_upd == 2 ? u2 : E.nyn[idx]));
+            const double q = cabs2d(ev) / (E.atol + E.rtol * fmax(cabs2d(y), cabs2d(yn)));
+            nloc += q * q;
+          }
         }
       }
-    }
-    if (P.last && P.herm_tiles) {
-      // off-diagonal block: write the conjugate-transposed block (J, I) of
-      // every output; diagonal block: rewrite its strictly lower triangle as
-      // the conjugate of the upper one and zero the imaginary part of its
-      // diagonal, so the state stays exactly Hermitian.  Through the tile
-      // buffer: element (r, c) staged at c*64 + (r ^ c), so that both the
-      // staging stores and the transposed reads are conflict-free
+    } else {
+      // Hermitian blocks: every output is written at its own position and,
+      // through the tile buffer, conjugate-transposed at block (J, I); a
+      // diagonal block rewrites its strictly lower triangle as the conjugate
+      // of the upper one and zeroes the imaginary part of its diagonal, so
+      // the state stays exactly Hermitian.  Element (r, c) is staged at
+      // c*64 + (r ^ c): both the staging stores and the transposed reads are
+      // conflict-free.
       double2 *stg = cur;
-      double2 *dst[4];
-      int nd = 0;
-      if (E.kout) dst[nd++] = E.kout;
-      for (int u = 0; u < E.nupd; u++) dst[nd++] = E.out[u];
+      const int nd = (E.kout ? 1 : 0) + E.nupd;
       for (int o = 0; o < nd; o++) {
-        __syncthreads();
+        const int u = E.kout ? o - 1 : o;
+        double2 *dst = u < 0 ? E.kout : E.out[u];
+        __syncthreads();  // the tile (o == 0) or the previous staging has been read
 #pragma unroll
         for (int i = 0; i < 2; i++)
 #pragma unroll
-          for (int m = 0; m < MC; m++)
-            stg[cl[m] * 64 + (rl[i] ^ cl[m])] = dst[o][(size_t)c[m] * D + r[i]];
+          for (int m = 0; m < QMC; m++) {
+            const size_t idx = (size_t)c[m] * D + r[i];
+            const double2 Kv = make_double2((double)acc[i][m].x, (double)acc[i][m].y);
+            const double2 b0 = u == 0 || E.yn_upd == 0 ? base0(i, m, idx) : make_double2(0.0, 0.0);
+            const double2 v = u < 0 ? Kv : stage_value(E, u, idx, Kv, b0);
+            dst[idx] = v;
+            stg[cl[m] * 64 + (rl[i] ^ cl[m])] = v;
+            if (E.nsum && u == E.err_upd) {
+              const double2 y = E.ny[idx];
+              const double2 yn = E.yn_upd >= 0 ? stage_value(E, E.yn_upd, idx, Kv, b0) : E.nyn[idx];
+              const double q = cabs2d(v) / (E.atol + E.rtol * fmax(cabs2d(y), cabs2d(yn)));
+              nloc += mirror ? 2.0 * q * q : q * q;
+            }
+          }
         __syncthreads();
-        for (int e2 = threadIdx.x; e2 < NEL; e2 += PT) {
+        for (int e2 = threadIdx.x; e2 < NEL; e2 += QT) {
           const unsigned a = e2 & 63u, b = e2 >> 6;
           double2 v = stg[a * 64 + (b ^ a)];  // value at (row b, column a) of block (I, J)
           v.y = -v.y;
-          if (mirror || a > b) dst[o][(size_t)(rfix | b) * D + (cfix | a)] = v;
-          else if (a == b) dst[o][(size_t)(rfix | b) * D + (cfix | a)] = make_double2(v.x, 0.0);
+          if (mirror || a > b) dst[(size_t)(rfix | b) * D + (cfix | a)] = v;
+          else if (a == b) dst[(size_t)(rfix | b) * D + (cfix | a)] = make_double2(v.x, 0.0);
         }
       }
     }
     __syncthreads();  // every thread is done with cur before it is refilled
+    if (!TMA) t_static += gridDim.x;
   }
   if (!TMA) cp_wait<0>();
+  if (TMA && threadIdx.x == 0) {
+    if (timed_out) {
+      // no new loads were issued after the time-out; give every load still
+      // outstanding (this stage and the two prefetched ones) a bounded wait
+      // so the CTA does not exit with copies in flight (if these waits run
+      // out as well, it exits anyway and the error word reports the run)
+      if (P.errflag) atomicExch(P.errflag, 1);
+      for (int k2 = 0; k2 < nst; k2++) {
+        const int q = (it + k2) % nst;
+        if (tids[q] < P.ntiles) mbar_wait_bounded(&bars[q], (unsigned)(((it + k2) / nst) & 1), 500000000ull);
+      }
+      if (bt) mbar_wait_bounded(&bars[3], (unsigned)(it & 1), 500000000ull);
+    }
+    // queue reset by the last CTA: every CTA has made its final claim
+    // before it counts itself here
+    __threadfence();
+    if (atomicAdd(P.done, 1u) == gridDim.x - 1) {
+      atomicExch(P.claim, 0ull);
+      atomicExch(P.done, 0u);
+    }
+  }
   if (P.last && E.nsum) {
     for (int o = 16; o > 0; o >>= 1) nloc += __shfl_down_sync(0xffffffffu, nloc, o);
     if (lane == 0) red[w] = nloc;
     __syncthreads();
     if (threadIdx.x == 0) {
       double s = 0.0;
-      for (int q = 0; q < PT / 32; q++) s += red[q];
+      for (int q = 0; q < QNW; q++) s += red[q];
       atomicAdd(E.nsum, s);
     }
-  }
-}
-
-// First pass (high six bits) when the last pass runs on the blocks I <= J
-// only: the running sum is needed just where the row's high bits do not
-// exceed the column's, i.e. on the upper triangle of every 64 x 64 tile of
-// this pass (2080 of 4096 outputs).  Canonical single-bit terms only.
-// Outputs are enumerated column by column over folded column pairs
-// (c, 63 - c): 65 per pair, consecutive threads on consecutive rows.
-template <int NTHR, int CANON, bool F32>
-__global__ void __launch_bounds__(NTHR, 1) k_qpass_hh(const __grid_constant__ PassParams P,
-                                                      const __grid_constant__ CUtensorMap tmap,
-                                                      const double2 *__restrict__ X) {
-  constexpr int PT = NTHR;
-  constexpr int NUP = 2080;
-  using V2 = typename std::conditional<F32, float2, double2>::type;
-  using S = typename std::conditional<F32, float, double>::type;
-  extern __shared__ __align__(128) double2 sm[];
-  __shared__ __align__(8) uint64_t bars[3];
-  const int n = P.n, lo = P.lo;
-  const size_t D = (size_t)1 << n;
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < 3; q++) mbar_init(&bars[q], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < 2; q++) {
-      const long long tq = blockIdx.x + (long long)q * gridDim.x;
-      if (tq < P.ntiles) tma_tile(P, &tmap, sm + q * NEL, &bars[q], tq);
-    }
-  }
-  constexpr bool C_HL = CANON < 0 || (CANON & 1), C_HR = CANON < 0 || (CANON & 2);
-  constexpr bool C_GL = CANON < 0 || (CANON & 4), C_GU = CANON < 0 || (CANON & 8);
-  long long t = blockIdx.x;
-  for (int it = 0; t < P.ntiles; it++, t += gridDim.x) {
-    double2 *cur = sm + (it % 3) * NEL;
-    const long long t2 = t + 2ll * gridDim.x;
-    if (threadIdx.x == 0 && t2 < P.ntiles) tma_tile(P, &tmap, sm + ((it + 2) % 3) * NEL, &bars[(it + 2) % 3], t2);
-    const unsigned parity = (unsigned)((it / 3) & 1);
-    const unsigned long long t0 = global_ns();
-    bool timed_out = false;
-    while (!mbar_try_wait(&bars[it % 3], parity)) {
-      if (global_ns() - t0 > 2000000000ull) { timed_out = true; break; }
-    }
-    if (__syncthreads_or(timed_out)) {
-      if (threadIdx.x == 0 && P.errflag) atomicExch(P.errflag, 1);
-      return;
-    }
-    const V2 *tile = reinterpret_cast<const V2 *>(cur);
-    if (F32) {
-      double2 tmp[NEL / PT];
-#pragma unroll
-      for (int k2 = 0; k2 < NEL / PT; k2++) tmp[k2] = cur[threadIdx.x + k2 * PT];
-      __syncthreads();
-      float2 *c32 = reinterpret_cast<float2 *>(cur);
-#pragma unroll
-      for (int k2 = 0; k2 < NEL / PT; k2++)
-        c32[threadIdx.x + k2 * PT] = make_float2((float)tmp[k2].x, (float)tmp[k2].y);
-      __syncthreads();
-    }
-    unsigned rfix, cfix;
-    tile_origin(t, n, lo, rfix, cfix);
-    V2 *aout = reinterpret_cast<V2 *>(P.accout);
-    for (int e = threadIdx.x; e < NUP; e += PT) {  // NUP is a multiple of 32: whole warps
-      const int fc = e / 65, p = e - fc * 65;
-      unsigned rr, cc;
-      if (p < 64 - fc) { rr = (unsigned)p; cc = (unsigned)(63 - fc); }
-      else { rr = (unsigned)(p - (64 - fc)); cc = (unsigned)fc; }
-      S ax = 0, ay = 0;
-#pragma unroll
-      for (int b = 0; b < 6; b++) {
-        const unsigned f = 1u << b;
-        if (C_HL) {
-          const S hl = (S)P.hl[b];
-          const V2 q = tile[cc * 64 + (rr ^ f)];
-          ax = fma(-hl, q.y, ax);
-          ay = fma(hl, q.x, ay);
-        }
-        if (C_HR) {
-          const S hr = (S)P.hr[b];
-          const V2 q = tile[(cc ^ f) * 64 + rr];
-          ax = fma(-hr, q.y, ax);
-          ay = fma(hr, q.x, ay);
-        }
-        if (C_GL || C_GU) {
-          const bool rb = rr & f, cb = cc & f;
-          const S g = (rb != cb) ? (S)0 : (rb ? (C_GU ? (S)P.gu[b] : (S)0) : (C_GL ? (S)P.gl[b] : (S)0));
-          const V2 q = tile[(cc ^ f) * 64 + (rr ^ f)];
-          ax = fma(g, q.x, ax);
-          ay = fma(g, q.y, ay);
-        }
-      }
-      V2 v;
-      v.x = ax;
-      v.y = ay;
-      aout[(size_t)(cfix | (cc << lo)) * D + (rfix | (rr << lo))] = v;
-    }
-    __syncthreads();  // every thread is done with cur before it is refilled
   }
 }
 
@@ -715,48 +714,52 @@ void encode_tma(const PassParams &pp, const double2 *x, CUtensorMap *map) {
   if (r != CUDA_SUCCESS) fail(9, "ERROR! cuTensorMapEncodeTiled failed (%d)\n", (int)r);
 }
 
-template <bool REAL, bool TMA, int NTHR, int CANON, bool F32>
-void launch_pass(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e,
-                 int grid, size_t smem, cudaStream_t s) {
-  ensure_smem((const void *)k_qpass<REAL, TMA, NTHR, CANON, F32>, smem);
-  k_qpass<REAL, TMA, NTHR, CANON, F32><<<grid, NTHR, smem, s>>>(pp, map, x, e);
+template <bool REAL, bool TMA, int CANON, bool F32>
+void launch_pass(const PassParams &pp, const CUtensorMap &map, const CUtensorMap &bmap, const double2 *x,
+                 const Epi &e, int grid, size_t smem, cudaStream_t s, bool dry) {
+  ensure_smem((const void *)k_qpass<REAL, TMA, CANON, F32>, smem);
+  if (dry) {
+    cudaFuncAttributes fa;
+    QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_qpass<REAL, TMA, CANON, F32>));
+    return;
+  }
+  k_qpass<REAL, TMA, CANON, F32><<<grid, QT, smem, s>>>(pp, map, bmap, x, e);
 }
 
 template <bool F32>
 struct Canon {
   template <int CANON>
-  static void launch(const PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e, int grid,
-                     size_t smem, cudaStream_t s) {
-    launch_pass<true, true, 1024, CANON, F32>(pp, map, x, e, grid, smem, s);
+  static void launch(const PassParams &pp, const CUtensorMap &map, const CUtensorMap &bmap, const double2 *x,
+                     const Epi &e, int grid, size_t smem, cudaStream_t s, bool dry) {
+    launch_pass<true, true, CANON, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
   }
 };
 
 // canonical fast path: real mode, TMA, no general terms in this pass
 template <bool F32>
-void launch_canon_mask(int mask, const PassParams &pp, const CUtensorMap &map, const double2 *x,
-                       const Epi &e, int grid, size_t smem, cudaStream_t s) {
+void launch_canon_mask(int mask, const PassParams &pp, const CUtensorMap &map, const CUtensorMap &bmap,
+                       const double2 *x, const Epi &e, int grid, size_t smem, cudaStream_t s, bool dry) {
 #define launch_canon Canon<F32>::template launch
   switch (mask) {
-    case 0: launch_canon<0>(pp, map, x, e, grid, smem, s); break;
-    case 1: launch_canon<1>(pp, map, x, e, grid, smem, s); break;
-    case 2: launch_canon<2>(pp, map, x, e, grid, smem, s); break;
-    case 3: launch_canon<3>(pp, map, x, e, grid, smem, s); break;
-    case 4: launch_canon<4>(pp, map, x, e, grid, smem, s); break;
-    case 5: launch_canon<5>(pp, map, x, e, grid, smem, s); break;
-    case 6: launch_canon<6>(pp, map, x, e, grid, smem, s); break;
-    case 7: launch_canon<7>(pp, map, x, e, grid, smem, s); break;
-    case 8: launch_canon<8>(pp, map, x, e, grid, smem, s); break;
-    case 9: launch_canon<9>(pp, map, x, e, grid, smem, s); break;
-    case 10: launch_canon<10>(pp, map, x, e, grid, smem, s); break;
-    case 11: launch_canon<11>(pp, map, x, e, grid, smem, s); break;
-    case 12: launch_canon<12>(pp, map, x, e, grid, smem, s); break;
-    case 13: launch_canon<13>(pp, map, x, e, grid, smem, s); break;
-    case 14: launch_canon<14>(pp, map, x, e, grid, smem, s); break;
-    default: launch_canon<15>(pp, map, x, e, grid, smem, s); break;
+    case 0: launch_canon<0>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 1: launch_canon<1>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 2: launch_canon<2>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 3: launch_canon<3>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 4: launch_canon<4>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 5: launch_canon<5>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 6: launch_canon<6>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 7: launch_canon<7>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 8: launch_canon<8>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 9: launch_canon<9>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 10: launch_canon<10>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 11: launch_canon<11>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 12: launch_canon<12>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 13: launch_canon<13>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    case 14: launch_canon<14>(pp, map, bmap, x, e, grid, smem, s, dry); break;
+    default: launch_canon<15>(pp, map, bmap, x, e, grid, smem, s, dry); break;
   }
 #undef launch_canon
 }
-
 
 int canon_mask(const PassParams &pp) {
   int m = 0;
@@ -770,28 +773,33 @@ int canon_mask(const PassParams &pp) {
 }
 
 template <bool F32>
-void launch_any_pass(PassParams &pp, const CUtensorMap &map, const double2 *x, const Epi &e, int grid,
-                     size_t smem, cudaStream_t s) {
+void launch_any_pass(const PassParams &pp, const CUtensorMap &map, const CUtensorMap &bmap, const double2 *x,
+                     const Epi &e, int grid, size_t smem, cudaStream_t s, bool dry) {
   const bool tma = pp.tma != 0;
   const bool only_canon = pp.real && tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 &&
                           pp.nspill == 0;
-  if (only_canon) launch_canon_mask<F32>(canon_mask(pp), pp, map, x, e, grid, smem, s);
-  else if (pp.real && tma) launch_pass<true, true, 512, -1, F32>(pp, map, x, e, grid, smem, s);
-  else if (pp.real) launch_pass<true, false, 512, -1, F32>(pp, map, x, e, grid, smem, s);
-  else if (tma) launch_pass<false, true, 512, -1, F32>(pp, map, x, e, grid, smem, s);
-  else launch_pass<false, false, 512, -1, F32>(pp, map, x, e, grid, smem, s);
+  if (only_canon) launch_canon_mask<F32>(canon_mask(pp), pp, map, bmap, x, e, grid, smem, s, dry);
+  else if (pp.real && tma) launch_pass<true, true, -1, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
+  else if (pp.real) launch_pass<true, false, -1, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
+  else if (tma) launch_pass<false, true, -1, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
+  else launch_pass<false, false, -1, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
 }
 
-template <int CANON, bool F32>
-void launch_hh(const PassParams &pp, const CUtensorMap &map, const double2 *x, int grid, size_t smem,
-               cudaStream_t s) {
-  ensure_smem((const void *)k_qpass_hh<1024, CANON, F32>, smem);
-  k_qpass_hh<1024, CANON, F32><<<grid, 1024, smem, s>>>(pp, map, x);
+// A pass whose terms are canonical single-bit ones that map Hermitian
+// inputs to Hermitian outputs (left and right X with opposite
+// coefficients, real jumps): its tile (b, a) result is the conjugate
+// transpose of its tile (a, b) result.
+bool hermitian_canonical_pass(const PassParams &pp) {
+  if (!(pp.real && pp.tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 && pp.nspill == 0 &&
+        !pp.diag))
+    return false;
+  for (int b = 0; b < 6; b++)
+    if (pp.hl[b] != -pp.hr[b]) return false;
+  return true;
 }
 
-bool canonical_only(const PassParams &pp) {
-  return pp.real && pp.tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 && pp.nspill == 0 &&
-         !pp.diag;
+size_t pass_smem(const PassParams &pp) {
+  return (size_t)((pp.tma ? 3 : 2) * NEL + QMAX_GROUPS * 64) * sizeof(double2);
 }
 
 }  // namespace
@@ -897,6 +905,8 @@ bool plan_qubit_passes(const DeviceProgram &P, std::vector<PassParams> &out) {
     for (size_t i = 0; i < all.size(); i++) pp.t[i] = all[i];
     pp.tma = describe_tma(pp) ? 1 : 0;
     pp.errflag = P.errflag;
+    pp.claim = P.tile_claim;
+    pp.done = P.tile_done;
     out.push_back(pp);
   }
   return true;
@@ -908,7 +918,9 @@ bool check_program_error(DeviceProgram &P, cudaStream_t s) {
   QCUDA(cudaMemcpyAsync(&h, P.errflag, sizeof(int), cudaMemcpyDeviceToHost, s));
   QCUDA(cudaStreamSynchronize(s));
   if (h) {
-    QCUDA(cudaMemsetAsync(P.errflag, 0, sizeof(int), s));
+    // error word and tile-queue words start again from zero
+    QCUDA(cudaMemsetAsync(P.errflag, 0, 16, s));
+    QCUDA(cudaStreamSynchronize(s));
     fail(9, "ERROR! a tile load did not complete within its time limit; results are invalid\n");
     return false;
   }
@@ -922,43 +934,60 @@ static std::atomic<int64_t> g_herm_applications{0};
 void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, double2 *scratch,
                          const Epi &e, cudaStream_t s, bool f32) {
   const int np = (int)passes.size();
-  const long long nt = passes[0].ntiles;
-  const int grid = (int)std::min<long long>(nt, num_sms());
-  // Hermitian mode: two passes whose first covers exactly bits 6..11 (12 qubits)
-  const bool herm = e.herm && np == 2 && passes[0].lo == 6 && passes[0].n == 12 && canonical_only(passes[0]) &&
-                    passes[1].lo == 0 && passes[1].last;
+  const int n = passes[0].n;
+  // Hermitian mode: the last pass (low group) works on the blocks I <= J of
+  // the bits above it and mirrors them; a two-pass program whose first pass
+  // is a Hermitian canonical pass over the top six bits runs that pass on
+  // tile pairs
+  const bool herm = e.herm && passes.back().lo == 0 && passes.back().last;
+  const bool pair = herm && np == 2 && passes[0].lo + 6 == n && hermitian_canonical_pass(passes[0]);
   if (herm) g_herm_applications++;
+  const long long T = 1ll << (n - 6);
   for (int p = 0; p < np; p++) {
     PassParams &pp = passes[p];
     pp.accin = p > 0 ? scratch : nullptr;
     pp.accout = (p < np - 1) ? scratch : nullptr;
     const long long ntiles_full = pp.ntiles;
-    if (herm && p == 1) {
-      const long long T = 1ll << (pp.n - 6);
+    if (herm && p == np - 1) {
       pp.herm_tiles = 1;
       pp.ntiles = T * (T + 1) / 2;
     }
-    CUtensorMap map;
-    memset(&map, 0, sizeof(map));
-    const bool tma = pp.tma != 0;
-    if (tma) encode_tma(pp, x, &map);
-    const size_t smem = (size_t)((tma ? 3 : 2) * NEL + QMAX_GROUPS * 64) * sizeof(double2);
-    const int g = (int)std::min<long long>(pp.ntiles, num_sms());
-    if (herm && p == 0) {
-      const bool m7 = canon_mask(pp) == 7;
-      if (f32) { if (m7) launch_hh<7, true>(pp, map, x, g, smem, s); else launch_hh<-1, true>(pp, map, x, g, smem, s); }
-      else { if (m7) launch_hh<7, false>(pp, map, x, g, smem, s); else launch_hh<-1, false>(pp, map, x, g, smem, s); }
-    } else if (f32) {
-      launch_any_pass<true>(pp, map, x, e, g, smem, s);
-    } else {
-      launch_any_pass<false>(pp, map, x, e, g, smem, s);
+    if (pair && p == 0) {
+      pp.pair_tiles = 1;
+      pp.ntiles = T * (T + 1) / 2;
     }
+    CUtensorMap map, bmap;
+    memset(&map, 0, sizeof(map));
+    memset(&bmap, 0, sizeof(bmap));
+    if (pp.tma) encode_tma(pp, x, &map);
+    // the kernel loads the first stage base by TMA in a last pass with TMA
+    if (pp.tma && pp.last && e.nupd > 0 && e.base[0]) encode_tma(pp, e.base[0], &bmap);
+    const int g = (int)std::min<long long>(pp.ntiles, num_sms());
+    if (f32) launch_any_pass<true>(pp, map, bmap, x, e, g, pass_smem(pp), s, false);
+    else launch_any_pass<false>(pp, map, bmap, x, e, g, pass_smem(pp), s, false);
     pp.herm_tiles = 0;
+    pp.pair_tiles = 0;
     pp.ntiles = ntiles_full;
     count_launch();
     QCUDA(cudaGetLastError());
   }
-  (void)grid;
+}
+
+void preload_lrho_kernels(const DeviceProgram &P) {
+  if (P.has_qubit && !P.passes.empty()) {
+    CUtensorMap map;
+    memset(&map, 0, sizeof(map));
+    Epi e;
+    zero_epi(e);
+    for (const PassParams &pp : P.passes) {
+      launch_any_pass<false>(pp, map, map, nullptr, e, 1, pass_smem(pp), 0, true);
+      launch_any_pass<true>(pp, map, map, nullptr, e, 1, pass_smem(pp), 0, true);
+    }
+  } else if (P.has_qubit) {
+    preload_single_pass_qubit_kernels();
+  } else {
+    preload_generic_lrho_kernels();
+  }
 }
 
 }  // namespace quac

@@ -238,6 +238,14 @@ void launch_q(const QParams &qp, const double2 *x, const Epi &e, cudaStream_t s)
 
 }  // namespace
 
+void preload_single_pass_qubit_kernels() {
+  cudaFuncAttributes fa;
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho_qubit<4, true>));
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho_qubit<4, false>));
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho_qubit<8, true>));
+  QCUDA(cudaFuncGetAttributes(&fa, (const void *)k_lrho_qubit<8, false>));
+}
+
 void launch_lrho_qubit(const DeviceProgram &P, const double2 *x, const Epi &e, cudaStream_t s) {
   static QParams qp;  // assembled on the host per launch (5-6 KB parameter block)
   qp.prog = P.qdev;

@@ -12,8 +12,13 @@
 //     scratch: a 10-qubit density matrix); larger systems are rejected;
 //   - quac_lrho_noalloc_setup must be called once per system, with the
 //     system's device current, before the first apply and before any stream
-//     capture: it compiles the term program if needed and looks up the
-//     scratch address of the current device;
+//     capture: it compiles the term program if needed, looks up the scratch
+//     address of the current device and loads every kernel the apply can
+//     launch (CUDA's lazy module loading would otherwise load, and allocate
+//     device memory for, a kernel at its first launch);
+//   - the apply follows quac_set_lrho_precision like quac_lrho_apply_device
+//     (complex128 or complex64 contraction) and returns once the result is
+//     complete;
 //   - the scratch is shared by every system on a device: calls that overlap
 //     in time (two host threads, or two streams) race on it and give wrong
 //     results; serialise them.
@@ -57,11 +62,17 @@ extern "C" int quac_lrho_noalloc_setup(qsystem qs) {
   g_scratch_of_device[dev].store((double2 *)addr);
   stream_of(qs);
   ensure_program(qs);
+  if (has_error() || !qs->impl->prog) return 1;
+  preload_lrho_kernels(*qs->impl->prog);
   return has_error() ? 1 : 0;
 }
 
 extern "C" int quac_lrho_apply_device_noalloc(qsystem qs, const void *x_dev, void *y_dev) {
   if (qs->mat_allocated != 1) { fail(0, "ERROR! call construct_matrix first\n"); return 1; }
+  if (!qs->impl->td.empty()) {
+    fail(0, "ERROR! quac_lrho_apply_device_noalloc: time-dependent terms need quac_lrho_apply_device\n");
+    return 1;
+  }
   const int mode = qs->dm_equations ? 0 : 1;
   if (!qs->impl->prog || qs->impl->prog_mode != mode) {
     fail(0, "ERROR! call quac_lrho_noalloc_setup on this system before quac_lrho_apply_device_noalloc\n");
@@ -87,7 +98,8 @@ extern "C" int quac_lrho_apply_device_noalloc(qsystem qs, const void *x_dev, voi
     // the first pass writes the running sum without reading it, so only the
     // time-limit error word has to start at zero
     if (P.errflag) QCUDA(cudaMemsetAsync(P.errflag, 0, sizeof(int), s));
-    launch_qubit_passes(P.passes, (const double2 *)x_dev, g_scratch_of_device[dev].load(), e, s);
+    launch_qubit_passes(P.passes, (const double2 *)x_dev, g_scratch_of_device[dev].load(), e, s,
+                        options().lrho_f32 != 0);
   } else {
     // the single-pass kernels use no scratch
     launch_lrho_any(P, (const double2 *)x_dev, e, s);

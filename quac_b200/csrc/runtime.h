@@ -29,6 +29,19 @@ struct Term {
   std::vector<op_handle> ops;
 };
 
+struct DeviceProgram;
+// A time-dependent term: its superoperator with coefficient 1, scaled by
+// a f(t) at every stage (qsystem.c:1300-1330)
+struct TdTerm {
+  Term term;                                // term.a = the caller's coefficient
+  quac_time_dep_func f = nullptr;           // one of the two callback forms
+  quac_time_dep_func_parts g = nullptr;
+  void *ctx = nullptr;
+  DeviceProgram *prog = nullptr;
+  int prog_mode = -1;
+  cplx scale(double t) const;
+};
+
 struct Options {
   std::string rk_type = "3bs";
   std::string adapt_type = "basic";
@@ -66,11 +79,19 @@ struct qsystem_impl {
   quac::Workspace ws;
   std::vector<op_handle> owned_ops;  // every operator struct created for this system
   Vec host_vec = nullptr;            // device state of quac_time_step_host, kept between calls
+  std::vector<quac::TdTerm> td;      // time-dependent terms
+  double2 *td_acc = nullptr;         // L(t) x and one term's contribution (2 x dim, lazily allocated)
+  int64_t td_acc_n = 0;
 };
 
 namespace quac {
 cudaStream_t stream_of(qsystem qs);
 void ensure_program(qsystem qs);
+// y-side of one RK stage at time t: the fused L.x launch for a
+// time-independent system; with time-dependent terms, L(t) x is summed
+// term group by term group and the epilogue runs as its own pass
+void apply_L(qsystem qs, double t, const double2 *x, const Epi &e, cudaStream_t s);
+void release_td_programs(qsystem qs);
 int64_t vec_len(Vec v);
 void vec_sync_to_device(Vec v);       // flush pending host additions
 Vec vec_new(int64_t n);

@@ -1370,6 +1370,7 @@ using namespace quac;
 
 extern "C" PetscInt steady_state_sys(qsystem qs, qvec x) {
   if (!qs->dm_equations) { fail(0, "ERROR! steady_state_sys needs Lindblad terms\n"); return -1; }
+  if (!qs->impl->td.empty()) { fail(0, "ERROR! a steady state needs a time-independent system\n"); return -1; }
   if (!qs->mat_allocated) construct_matrix(qs);
   if (has_error()) return -1;
   vec_sync_to_device(x->data);
@@ -1400,6 +1401,7 @@ static Deflation &deflation_slot() {
 extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScalar *U_host, PetscInt kd,
                                              PetscInt maxit_guided, PetscReal *residual) {
   if (!qs->dm_equations) { fail(0, "ERROR! steady state needs Lindblad terms\n"); return -1; }
+  if (!qs->impl->td.empty()) { fail(0, "ERROR! a steady state needs a time-independent system\n"); return -1; }
   if (kd < 0 || kd > KDMAX) { fail(0, "ERROR! deflation rank must be in [0, %d]\n", KDMAX); return -1; }
   if (!qs->mat_allocated) construct_matrix(qs);
   if (has_error()) return -1;

@@ -104,6 +104,8 @@ void DeviceProgram::release() {
   allocations.clear();
   scratch = nullptr;
   errflag = nullptr;
+  tile_done = nullptr;
+  tile_claim = nullptr;
 }
 
 namespace {
@@ -321,11 +323,16 @@ DeviceProgram *compile_terms(qsystem qs, int mode) {
   d.qubit_path = 0;
   if (options().kernel_path != 1 && mode == 0) compile_qubit(qs, hp, P);
   if (P->has_qubit && options().kernel_path != 2) {
-    QCUDA(cudaMalloc(&P->errflag, sizeof(int)));
-    QCUDA(cudaMemset(P->errflag, 0, sizeof(int)));
-    P->allocations.push_back(P->errflag);
+    // one 16-byte block: error word, tile-queue done counter, tile claim counter
+    char *words = nullptr;
+    QCUDA(cudaMalloc(&words, 16));
+    QCUDA(cudaMemset(words, 0, 16));
+    P->allocations.push_back(words);
+    P->errflag = (int *)words;
+    P->tile_done = (unsigned *)(words + 4);
+    P->tile_claim = (unsigned long long *)(words + 8);
     if (!plan_qubit_passes(*P, P->passes)) P->passes.clear();
-    if (P->passes.size() == 2) P->herm_ok = hermiticity_preserving(hp);
+    if (!P->passes.empty()) P->herm_ok = hermiticity_preserving(hp);
   }
   d.qubit_path = P->has_qubit ? 1 : 0;
   return P;

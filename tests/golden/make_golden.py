@@ -2,7 +2,7 @@
 
 Run once in a container where the reference tree is mounted:
 
-    python tests/golden/make_golden.py /root/reference/tests/pristine_matrices
+    python tests/golden/make_golden.py <reference checkout>/tests/pristine_matrices
 
 It writes tests/golden/pristine.npz.  The fixtures are the golden
 superoperator matrices and state vectors used by the reference's
@@ -48,10 +48,15 @@ def main(src):
         for k, v in d.items():
             out[f"{key}__{k}"] = v
         out[f"{key}__kind"] = np.array(kind)
+        if kind == "vec":
+            # the file's own bytes, for reading through the library's PETSc-binary reader
+            out[f"{key}__raw"] = np.frombuffer(open(os.path.join(src, name), "rb").read(), dtype=np.uint8)
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pristine.npz")
     np.savez_compressed(dst, **out)
     print(f"wrote {dst} ({len(out)} arrays)")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests/pristine_matrices")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference>/tests/pristine_matrices")
+    main(sys.argv[1])

@@ -1,0 +1,264 @@
+"""Benchmark configurations end to end against the oracle, and the qvec /
+legacy entry points around them (run on a B200: pytest -m gpu).
+
+  config 1  Jaynes-Cummings 2 x 10, fixed RK4 dt = 0.01 to t = 200 with the
+            populations read every step (the simple_jc_test monitor form)
+  config 2  noisy 10-qubit random circuit: superoperator gates and 1.0 time
+            unit of adaptive BS3 per layer, fidelity against the ideal state
+  config 3  complex64 contraction against the complex128 oracle (trace,
+            populations, fidelity), on the 8-qubit chain the oracle runs
+  legacy    create_op / add_to_ham / add_lin / steady_state(Vec) and
+            get_populations (operators.c, solver.c, dm_utilities.c)
+  qvec      read_qvec_dm_binary on the reference's rand_dm.dat, element
+            read-back, PETSc-binary write, set_qvec_from_init_excited_op,
+            get_bitstring_probs
+
+Bars: 1e-10 relative for complex128 integrations, 1e-12 for single reads.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _jc_pops(levels, x):
+    """(emitter, cavity) populations of a column-stacked JC state (emitter =
+    subsystem 0, the most significant digit)."""
+    D = int(np.prod(levels))
+    d = x.reshape(D, D, order="F").diagonal().real.reshape(levels)
+    return d[1, :].sum(), (d.sum(axis=0) * np.arange(levels[1])).sum()
+
+
+def test_config1_jc_rk4_t200_populations_match_oracle(quac, oracle):
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    qb, cav = H.jc(S)
+    H.jc(O)
+    quac.construct_matrix(S.qs)
+    rho = quac.create_qvec_sys(S.qs)
+    quac.add_to_qvec(rho, 1.0, 10, 10)
+    quac.assemble_qvec(rho)
+    got = {}
+
+    def monitor(step, t, vec):
+        if step % 1000 == 0:
+            got[step] = (quac.get_expectation_value_qvec(rho, qb.n).real,
+                         quac.get_expectation_value_qvec(rho, cav.n).real)
+
+    quac.set_ts_monitor_sys(S.qs, monitor)
+    quac.set_ts_options(rk_type="4", adapt_type="none")
+    try:
+        quac.time_step_sys(S.qs, rho, 0.0, 200.0, 0.01, 10 ** 6)
+    finally:
+        quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+        quac.set_ts_monitor_sys(S.qs, None)
+    assert sorted(got) == list(range(0, 20001, 1000))
+    h = O.csr_handle()
+    y = np.zeros(400, dtype=complex)
+    y[10 * 20 + 10] = 1.0
+    for step in range(0, 20001, 1000):
+        if step:
+            y = oracle.rk4(h, y, 0.01, 1000)
+        pe, pc = _jc_pops([2, 10], y)
+        ge, gc = got[step]
+        assert abs(ge - pe) <= 1e-10 * abs(pe) + 1e-14, (step, ge, pe)
+        assert abs(gc - pc) <= 1e-10 * abs(pc) + 1e-14, (step, gc, pc)
+    oracle.free_csr(h)
+    assert _rel(rho.to_numpy(), y) < 1e-10
+    rho.destroy()
+    S.qs.destroy()
+
+
+@pytest.mark.parametrize("layers", [5])
+def test_config2_noisy_circuit_matches_oracle(quac, oracle, layers):
+    """Each layer: the drawn gates on rho (superoperator convention) and 1.0
+    time unit of BS3 (dt0 = 0.1), both against the oracle step for step;
+    the state after every layer to 1e-10 and the fidelity against the ideal
+    (noiseless) state from both sides."""
+    from quac_b200.systems import noisy_circuit_layers, noisy_qubits
+    nq = 10
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    noisy_qubits(S, nq)
+    noisy_qubits(O, nq)
+    quac.construct_matrix(S.qs)
+    D = S.D
+    rho = quac.create_dm_sys(S.qs)
+    quac.add_to_qvec(rho, 1.0, 0, 0)
+    quac.assemble_qvec(rho)
+    spec = noisy_circuit_layers(nq, layers)
+    h = O.csr_handle()
+    y = np.zeros(D * D, dtype=complex)
+    y[0] = 1.0
+    ideal = y.copy()
+    levels = [2] * nq
+    t = 0.0
+    c0 = quac.hermitian_apply_count()
+    for layer in spec:
+        c = quac.create_circuit(len(layer))
+        for g, qbits, kw in layer:
+            c.add_gate(0.0, g, *qbits, **kw)
+            y = oracle.gate_superop(levels, y, g, list(qbits), **kw)
+            ideal = oracle.gate_superop(levels, ideal, g, list(qbits), **kw)
+        quac.apply_circuit_to_qvec(S.qs, c, rho)
+        quac.time_step_sys(S.qs, rho, t, t + 1.0, 0.1, 10 ** 6)
+        y, _, _ = oracle.bs3(h, y, t, t + 1.0, 0.1)
+        t += 1.0
+        got = rho.to_numpy()
+        assert _rel(got, y) < 1e-10
+        fid_gpu = float(np.vdot(ideal, got).real)
+        fid_orc = float(np.vdot(ideal, y).real)
+        assert abs(fid_gpu - fid_orc) < 1e-10
+    oracle.free_csr(h)
+    # the benchmarked path: these integrations ran in Hermitian mode
+    assert quac.hermitian_apply_count() > c0
+    assert 0.5 < fid_orc < 1.0
+    rho.destroy()
+    S.qs.destroy()
+
+
+def test_config3_fp32_contraction_errors_against_oracle(quac, oracle):
+    """The precision form of config 3 on the 8-qubit chain the oracle can
+    integrate: DP5 at rtol = atol = 1e-8 to t = 5 with complex64
+    contraction against the oracle's complex128 DP5, per result."""
+    n = 8
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.tfim(S, n)
+    H.tfim(O, n)
+    quac.construct_matrix(S.qs)
+    D = S.D
+    x0 = np.zeros(D * D, dtype=complex)
+    x0[0] = 1.0
+    out = {}
+    for prec in (0, 1):
+        rho = quac.create_dm_sys(S.qs)
+        rho.from_numpy(x0)
+        quac.set_lrho_precision(prec)
+        quac.set_ts_options(rk_type="5dp", adapt_type="basic", rtol=1e-8, atol=1e-8)
+        try:
+            quac.time_step_sys(S.qs, rho, 0.0, 5.0, 0.01, 10 ** 6)
+        finally:
+            quac.set_lrho_precision(0)
+            quac.set_ts_options(rk_type="3bs", adapt_type="basic", rtol=5e-7, atol=5e-7)
+        out[prec] = rho.to_numpy().reshape(D, D, order="F")
+        rho.destroy()
+    h = O.csr_handle()
+    yo, _, _ = oracle.dp5(h, x0, 0.0, 5.0, 0.01, atol=1e-8, rtol=1e-8)
+    oracle.free_csr(h)
+    Y = yo.reshape(D, D, order="F")
+    assert _rel(out[0], Y) < 1e-10
+    B = out[1]
+    # fidelity F = (Tr sqrt(sqrt(A) B sqrt(A)))^2 against the oracle state
+    w, V = np.linalg.eigh(Y)
+    sa = (V * np.sqrt(np.clip(w, 0, None))) @ V.conj().T
+    ev = np.linalg.eigvalsh(sa @ ((B + B.conj().T) / 2) @ sa)
+    fid = float(np.sum(np.sqrt(np.clip(ev, 0, None))) ** 2)
+    assert abs(np.trace(B) - np.trace(Y)) < 1e-6
+    assert np.abs(B.diagonal().real - Y.diagonal().real).max() < 1e-6
+    assert abs(fid - 1.0) < 1e-6
+
+
+def test_legacy_steady_state_matches_direct_solve(quac, oracle):
+    """steady_state(Vec) on the legacy global system (create_op, add_to_ham,
+    add_to_ham_mult2, add_lin; solver.c:33-221, operators.c:290-337,
+    679-719), with get_populations (dm_utilities.c:1157-1325)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    q = quac
+    qb = q.create_op(2)
+    cav = q.create_op(5)
+    q.add_to_ham(0.2, cav.n)
+    q.add_to_ham_mult2(0.1, cav.dag, qb)
+    q.add_to_ham_mult2(0.1, cav, qb.dag)
+    q.add_to_ham(0.15, cav)
+    q.add_to_ham(0.15, cav.dag)
+    q.add_lin(0.05, cav)
+    q.add_lin(2e-3, qb)
+    rho = q.create_full_dm()
+    q.steady_state(rho)
+    x = rho.to_numpy()
+    O = oracle.OSys()
+    oq, oc = O.op(2), O.op(5)
+    O.ham(0.2, oc.n)
+    O.ham(0.1, oc.dag, oq.a)
+    O.ham(0.1, oc.a, oq.dag)
+    O.ham(0.15, oc.a)
+    O.ham(0.15, oc.dag)
+    O.lin(0.05, oc.a)
+    O.lin(2e-3, oq.a)
+    L = O.liouvillian().tocsr()
+    D = 10
+    n = D * D
+    A = (L + sp.csr_matrix((np.eye(D).reshape(-1, order="F"), (np.zeros(n, int), np.arange(n))),
+                           shape=(n, n))).tocsc()
+    b = np.zeros(n, complex)
+    b[0] = 1.0
+    xs = spla.spsolve(A, b)
+    assert _rel(x, xs) < 1e-8
+    pops = q.get_populations(rho)
+    X = xs.reshape(D, D, order="F").diagonal().real.reshape(2, 5)
+    assert abs(pops[0] - X[1, :].sum()) < 1e-9
+    assert abs(pops[1] - (X.sum(axis=0) * np.arange(5)).sum()) < 1e-9
+    assert abs(q.get_dm_element(rho, 3, 3) - xs[3 * D + 3]) < 1e-9
+    rho.destroy()
+
+
+def test_read_reference_dm_binary_and_elements(quac, golden, tmp_path):
+    """read_qvec_dm_binary on the reference's own rand_dm.dat bytes and the
+    element read-back of qvec_utilities_tests.c:788-870 (column stacking:
+    element (1, 0) at vector index 1); print_qvec_file writes the same bytes."""
+    src = tmp_path / "rand_dm.dat"
+    src.write_bytes(golden["rand_dm_dat__raw"].tobytes())
+    dm = quac.read_qvec_dm_binary(str(src))
+    assert dm.n == 16
+    for (r, c), v in {(0, 0): 0.21986779173439994, (1, 0): -0.16336963153116132 - 0.05584012449039134j,
+                      (3, 1): 0.0056141822506085995 + 0.041200982904222694j,
+                      (3, 3): 0.25891270101644115}.items():
+        assert abs(quac.get_dm_element_qvec(dm, r, c) - v) < 1e-12
+        assert abs(quac.get_dm_element_qvec(dm, c, r) - np.conj(v)) < 1e-12
+    assert np.array_equal(dm.to_numpy(), golden["rand_dm_dat__val"])
+    out = tmp_path / "back.dat"
+    quac.print_qvec_file(dm, str(out))
+    assert out.read_bytes() == src.read_bytes()
+    probs = quac.get_bitstring_probs(dm)
+    assert np.allclose(probs, golden["rand_dm_dat__val"].reshape(4, 4, order="F").diagonal().real, atol=0)
+    dm.destroy()
+    wsrc = tmp_path / "rand_wf.dat"
+    wsrc.write_bytes(golden["rand_wf_dat__raw"].tobytes())
+    wf = quac.read_qvec_wf_binary(str(wsrc))
+    assert np.array_equal(wf.to_numpy(), golden["rand_wf_dat__val"])
+    assert np.allclose(quac.get_bitstring_probs(wf), np.abs(golden["rand_wf_dat__val"]) ** 2, atol=0)
+    wf.destroy()
+
+
+def test_set_qvec_from_init_excited_op(quac):
+    """qvec_utilities.c:2540-2566: the initial excitations of the subsystems
+    select one basis state through n_after strides (subsystem 0 = most
+    significant digit); a density matrix gets |i><i|."""
+    q = quac
+    qs = q.initialize_system()
+    a, b, c = q.create_op_sys(qs, 3), q.create_op_sys(qs, 2), q.create_op_sys(qs, 4)
+    q.add_lin_term(qs, 0.1, a)
+    q.set_init_excited_op(a, 2)
+    q.set_init_excited_op(b, 1)
+    q.set_init_excited_op(c, 3)
+    q.construct_matrix(qs)
+    rho = q.create_qvec_sys(qs)
+    q.set_qvec_from_init_excited_op(qs, rho)
+    q.assemble_qvec(rho)
+    i = 2 * (2 * 4) + 1 * 4 + 3
+    D = 24
+    x = rho.to_numpy()
+    assert x[i * D + i] == 1.0 and np.count_nonzero(x) == 1
+    assert q.get_dm_element_qvec(rho, i, i) == 1.0
+    rho.destroy()
+    qs.destroy()

@@ -559,3 +559,77 @@ def test_hermitian_mode_not_used_for_non_hermitian_state(quac):
     assert quac.hermitian_apply_count() == c0
     rho.destroy()
     S.qs.destroy()
+
+
+def _herm_state(D, seed):
+    """Hermitian (not necessarily positive) test state, cheap at any size."""
+    rng = np.random.default_rng(seed)
+    X = rng.normal(size=(D, D)) + 1j * rng.normal(size=(D, D))
+    return ((X + X.conj().T) / 2).reshape(-1, order="F")
+
+
+# Hermitian mode at every size with two or more passes: tile pairs in the
+# first pass (TFIM, canonical terms), general and cross-group terms in both
+# passes (pump), three passes (13 qubits)
+@pytest.mark.parametrize("n,build", [(7, tfim_real), (8, tfim_real), (10, tfim_real), (9, tfim_pump),
+                                     (11, tfim_pump), (13, tfim_real)],
+                         ids=["tfim7", "tfim8", "tfim10", "pump9", "pump11", "tfim13"])
+def test_hermitian_mode_all_sizes_matches_full_computation(quac, n, build):
+    outs, counts = [], []
+    x0 = None
+    for mode in (1, 0):
+        S = H.ProductSystem(quac)
+        build(S, n)
+        quac.construct_matrix(S.qs)
+        D = S.D
+        if x0 is None:
+            x0 = _herm_state(D, seed=23)
+        rho = quac.create_dm_sys(S.qs)
+        rho.from_numpy(x0)
+        quac.set_hermitian_mode(mode)
+        quac.set_ts_options(rk_type="4", adapt_type="none")
+        c0 = quac.hermitian_apply_count()
+        try:
+            quac.time_step_sys(S.qs, rho, 0.0, 0.03, 0.01, 10 ** 6)
+        finally:
+            quac.set_hermitian_mode(1)
+            quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+        counts.append(quac.hermitian_apply_count() - c0)
+        outs.append(rho.to_numpy())
+        rho.destroy()
+        S.qs.destroy()
+    assert counts[0] >= 12 and counts[0] % 4 == 0 and counts[1] == 0
+    assert _rel(outs[0], outs[1]) < 1e-12
+    D = 1 << n
+    y = outs[0].reshape(D, D, order="F")
+    assert np.array_equal(y, y.conj().T)
+
+
+def test_hermitian_mode_lx_d4096_matches_oracle_rows(quac, oracle):
+    """The benchmarked kernel path (12-qubit TFIM, Hermitian mode: tile
+    pairs in the high pass, blocks I <= J and their mirrors in the low pass)
+    against the oracle's assembled rows, for a low and a high column range
+    (the high one written entirely by the mirror epilogue)."""
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    H.tfim(S, 12)
+    H.tfim(O, 12)
+    quac.construct_matrix(S.qs)
+    D = S.D
+    x = _herm_state(D, seed=24)
+    quac.set_hermitian_mode(2)
+    c0 = quac.hermitian_apply_count()
+    try:
+        y = quac.lrho_apply_host(S.qs, x)
+    finally:
+        quac.set_hermitian_mode(1)
+    assert quac.hermitian_apply_count() == c0 + 1
+    for c_lo, c_hi in [(2, 5), (4000, 4004)]:
+        r0, r1 = c_lo * D, c_hi * D
+        Ablk = O.liouvillian(rows=(r0, r1))
+        assert _rel(y[r0:r1], Ablk @ x) < 1e-12
+    Y = y.reshape(D, D, order="F")
+    assert np.array_equal(Y, Y.conj().T)
+    yfull = quac.lrho_apply_host(S.qs, x)
+    assert _rel(y, yfull) < 1e-13
+    S.qs.destroy()

@@ -184,14 +184,16 @@ def run_reference(args, rank, world):
                 "reference algorithm timed instead"}))
 
 
-def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8):
+def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8, tol=5e-7):
     """Driven Jaynes-Cummings ensemble (4096 instances, n_c ~ U{5..40}, each
-    evolved to t = 100 with its own Dormand-Prince 5(4) step): solves/s of
-    the persistent batched kernel in FP64 and with complex64 right-hand-side
-    increments, against the plain path (time_step_sys, -ts_rk_type 5dp, one
-    system at a time) timed on a sample, and the population error of the
-    FP32-increment mode against the FP64 ensemble (which the parity tests
-    hold to the oracle at 1e-10)."""
+    evolved to t = 100 with its own Dormand-Prince 5(4) step at atol = rtol
+    = tol): solves/s of the persistent batched kernel in FP64 and with
+    complex64 right-hand-side increments (steps whose error estimate lies
+    within 0.5 of the accept threshold re-evaluated in complex128), against
+    the plain path (time_step_sys, -ts_rk_type 5dp, one system at a time)
+    timed on a sample, and the population error of the complex64 mode
+    against the FP64 ensemble (which the parity tests hold to the oracle at
+    1e-10)."""
     from quac_b200 import systems as Sy
     params = Sy.driven_jc_ensemble_params(n_inst)
     built = []
@@ -203,10 +205,10 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8):
     for qs in built:
         qs.destroy()
     rho0 = np.concatenate([Sy.excited_vacuum(p["nc"]) for p in params])
-    out = {"workload": f"driven_jc_ensemble_{n_inst}", "t_end": tmax, "controller": "DP5(4) atol=rtol=5e-7"}
+    out = {"workload": f"driven_jc_ensemble_{n_inst}", "t_end": tmax, "controller": f"DP5(4) atol=rtol={tol:g}"}
     states = {}
     for mode, name in ((0, "fp64"), (1, "fp32_rhs")):
-        E.set_options(precision=mode)
+        E.set_options(precision=mode, atol=tol, rtol=tol)
         E.set_states(rho0)
         E.run(0.0, 0.5, dt0)  # captures the graph
         E.set_states(rho0)
@@ -217,12 +219,15 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8):
         st = E.stats()
         out[name] = {"solves_per_s": n_inst / dt, "seconds": dt, "mean_steps": float(st[:, 1].mean()),
                      "shape": list(E.shape())}
+        if mode == 1:
+            red = E.redone_steps()
+            out[name]["redone_step_fraction"] = float(red.sum() / max(1.0, (st[:, 1] + st[:, 2]).sum()))
     pops = lambda x, i: E.state(x, i).diagonal().real
     err = np.array([np.abs(pops(states[0], i) - pops(states[1], i)).max() for i in range(n_inst)])
     out["fp32_rhs"]["pop_err_vs_fp64"] = {"median": float(np.median(err)), "p99": float(np.percentile(err, 99)),
                                           "max": float(err.max()), "frac_le_1e-8": float((err <= 1e-8).mean())}
     # plain path: one system at a time through time_step_sys
-    q.set_ts_options(rk_type="5dp", adapt_type="basic")
+    q.set_ts_options(rk_type="5dp", adapt_type="basic", rtol=tol, atol=tol)
     rng = np.random.default_rng(0)
     tp, perr = 0.0, 0.0
     for i in rng.choice(n_inst, size=plain_sample, replace=False):
@@ -237,7 +242,7 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8):
         D = 2 * p["nc"]
         perr = max(perr, float(np.abs(x.reshape(D, D, order="F").diagonal().real - pops(states[0], i)).max()))
         B.qs.destroy()
-    q.set_ts_options(rk_type="3bs", adapt_type="basic")
+    q.set_ts_options(rk_type="3bs", adapt_type="basic", rtol=5e-7, atol=5e-7)
     plain = plain_sample / tp
     out["plain_fp64_solves_per_s"] = plain
     out["plain_sample"] = plain_sample
@@ -301,27 +306,40 @@ def precision_summary(q, qs, rho, x0, stream, steps, segment):
 def jc_summary(q, t_end=200.0, dt=0.01):
     """Jaynes-Cummings (emitter 2 x cavity 10, QuaC's simple JC form): fixed
     RK4 dt = 0.01 to t = 200 (20,000 steps) with the emitter and cavity
-    populations recorded by a monitor after every step."""
+    populations recorded after every step: through the device-side
+    observable monitor (one-CTA kernel, values handed back in batches of
+    1000 steps) and, for comparison, through a host TS monitor called after
+    every step (simple_jc_test.c:76-90)."""
     from quac_b200.systems import Builder, jc
-    S = Builder(q)
-    qb, cav = jc(S)
-    q.construct_matrix(S.qs)
-    rho = q.create_qvec_sys(S.qs)
-    q.add_to_qvec(rho, 1.0, 10, 10)
-    q.assemble_qvec(rho)
-    pops = []
-    q.set_ts_monitor_sys(S.qs, lambda step, t, v: pops.append(
-        (q.get_expectation_value_qvec(rho, qb.n).real, q.get_expectation_value_qvec(rho, cav.n).real)))
-    q.set_ts_options(rk_type="4", adapt_type="none")
-    t0 = time.perf_counter()
-    q.time_step_sys(S.qs, rho, 0.0, t_end, dt, 10 ** 7)
-    sec = time.perf_counter() - t0
-    q.set_ts_options(rk_type="3bs", adapt_type="basic")
-    q.set_ts_monitor_sys(S.qs, None)
-    out = {"workload": "jc_2x10_rk4_t200_monitored", "steps": len(pops) - 1, "seconds": sec,
-           "steps_per_s": (len(pops) - 1) / sec, "final_populations": {"emitter": pops[-1][0], "cavity": pops[-1][1]}}
-    rho.destroy()
-    S.qs.destroy()
+    out = {"workload": "jc_2x10_rk4_t200_monitored", "steps": int(round(t_end / dt))}
+    for form in ("observable_monitor", "ts_monitor"):
+        S = Builder(q)
+        qb, cav = jc(S)
+        q.construct_matrix(S.qs)
+        rho = q.create_qvec_sys(S.qs)
+        q.add_to_qvec(rho, 1.0, 10, 10)
+        q.assemble_qvec(rho)
+        pops = []
+        if form == "observable_monitor":
+            q.set_observable_monitor(S.qs, [(qb.n,), (cav.n,)], lambda st, tm, v: pops.extend(v.real.tolist()),
+                                     batch=1000)
+        else:
+            q.set_ts_monitor_sys(S.qs, lambda step, t, v: pops.append(
+                (q.get_expectation_value_qvec(rho, qb.n).real, q.get_expectation_value_qvec(rho, cav.n).real)))
+        q.set_ts_options(rk_type="4", adapt_type="none")
+        t0 = time.perf_counter()
+        q.time_step_sys(S.qs, rho, 0.0, t_end, dt, 10 ** 7)
+        sec = time.perf_counter() - t0
+        q.set_ts_options(rk_type="3bs", adapt_type="basic")
+        q.set_ts_monitor_sys(S.qs, None)
+        q.set_observable_monitor(S.qs, None, None)
+        nrec = len(pops) if form == "observable_monitor" else len(pops) - 1
+        out[form] = {"seconds": sec, "steps_per_s": out["steps"] / sec, "records": nrec,
+                     "final_populations": {"emitter": pops[-1][0], "cavity": pops[-1][1]}}
+        rho.destroy()
+        S.qs.destroy()
+    out["steps_per_s"] = out["observable_monitor"]["steps_per_s"]
+    out["vs_ts_monitor"] = out["observable_monitor"]["steps_per_s"] / out["ts_monitor"]["steps_per_s"]
     return out
 
 
@@ -484,6 +502,7 @@ def run_ours(args, rank, world, local_rank):
         out["fp32_contraction"] = precision_summary(q, qs, rho, x0, stream, args.steps, segment)
         q.set_stream(qs, None)
         out["ensemble"] = ensemble_summary(q)
+        out["ensemble_tight"] = ensemble_summary(q, tol=1e-10)
         out["jc"] = jc_summary(q)
         out["circuit"] = circuit_summary(q)
         out["steady_state"] = steady_summary(q)
@@ -518,14 +537,21 @@ def run_profile(args):
         q.construct_matrix(S.qs)
         D = S.D
         if args.profile == "rk4":
+            q.set_stream(S.qs, torch.cuda.current_stream().cuda_stream)
             X = torch.randn(D, D, dtype=torch.complex128)
             X = (X + X.conj().T) / 2
             rho = q.create_dm_sys(S.qs)
             rho.from_numpy(X.T.contiguous().reshape(-1).numpy())  # column-stacked
             q.set_ts_options(rk_type="4", adapt_type="none")
-            q.time_step_sys(S.qs, rho, 0.0, DT * args.rk4_steps, DT, 10 ** 6)
-            torch.cuda.synchronize()
-            print(f"ok D={D} rk4 steps={args.rk4_steps} hermitian applications={q.hermitian_apply_count()}")
+            for rep in range(max(1, args.reps)):
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                ev0.record()
+                q.time_step_sys(S.qs, rho, 0.0, DT * args.rk4_steps, DT, 10 ** 6)
+                ev1.record()
+                torch.cuda.synchronize()
+                print(f"ok D={D} rk4 steps={args.rk4_steps} hermitian applications={q.hermitian_apply_count()} "
+                      f"{ev0.elapsed_time(ev1) / (4 * args.rk4_steps) * 1e3:.1f} us per L.rho")
             return
         x = torch.randn(D * D, dtype=torch.complex128, device="cuda")
         y = torch.empty_like(x)

@@ -297,6 +297,21 @@ int quac_lrho_apply_host(qsystem qsys, const PetscScalar *x_host, PetscScalar *y
  * serialised by the caller. */
 int quac_lrho_noalloc_setup(qsystem qsys);
 int quac_lrho_apply_device_noalloc(qsystem qsys, const void *x_dev, void *y_dev);
+/* Observable monitor (no reference counterpart: QuaC programs read
+ * populations in a TS monitor after every step, simple_jc_test.c:76-90).
+ * The expectation values Tr(O_k rho) of nobs operator products (product k
+ * is ops[sum_{j<k} nops[j] ...], as in get_expectation_value_qvec) are
+ * recorded on the GPU after every step of time_step_sys and passed to cb in
+ * batches of up to `batch` steps: cb(n, steps, times, values, ctx) with
+ * values[i * nobs + k] for step steps[i] at time times[i].  Small density
+ * matrices (D^2 <= 4096) integrated with fixed RK4 then run many steps per
+ * launch with the state in shared memory; other runs record the values
+ * with one reduction per observable and step.  cb = NULL removes the
+ * monitor. */
+typedef void (*quac_observable_monitor)(PetscInt nsteps, const PetscInt *steps, const PetscReal *times,
+                                        const PetscScalar *values, void *ctx);
+int quac_set_observable_monitor(qsystem qsys, PetscInt nobs, const PetscInt *nops, op_handle *ops,
+                                quac_observable_monitor cb, void *ctx, PetscInt batch);
 /* Batched ensembles (no reference counterpart: QuaC integrates one system
  * per time_step_sys call, qsystem.c:895-1098).  Many independent systems,
  * each built with the usual calls (initialize_system, create_op_sys,
@@ -327,6 +342,13 @@ int quac_ensemble_get_states(quac_ensemble ens, PetscScalar *rho);
 /* Integrates every instance from t0 to tmax (first step dt0); fails if an
  * instance hit the step limit or a non-finite error norm. */
 int quac_ensemble_run(quac_ensemble ens, double t0, double tmax, double dt0);
+/* complex64 mode: a step whose error estimate lies within `margin` of the
+ * accept threshold (|err - 1| < margin, default 0.5) is estimated again
+ * with complex128 stages, so the accept / reject decisions follow the
+ * complex128 ones; 0 turns the re-evaluation off. */
+int quac_ensemble_set_redo_margin(quac_ensemble ens, double margin);
+/* Steps of instance i re-evaluated in complex128 during the last run. */
+int64_t quac_ensemble_redone_steps(quac_ensemble ens, int64_t i);
 int quac_ensemble_get_stats(quac_ensemble ens, int64_t i, double *t, int64_t *steps, int64_t *rejected,
                             int *flags);
 /* Re(diag rho_i) of every instance, packed: D_0 values, then D_1, ... */

@@ -71,6 +71,11 @@ def lib():
         L.orc_gmres_ilu.restype = i64
         L.orc_gmres_ilu.argtypes = [vp, vp, dbl, ctypes.c_int, i64, ctypes.c_int]
         L.orc_num_threads.restype = ctypes.c_int
+        L.orc_mcwf.restype = ctypes.c_int
+        L.orc_mcwf.argtypes = [vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, vp, vp, ctypes.c_uint64, dbl, dbl,
+                               dbl, dbl, dbl, dbl, dbl, ctypes.c_int, i64, vp]
+        L.orc_mcwf_draw.restype = dbl
+        L.orc_mcwf_draw.argtypes = [ctypes.c_uint64, i64, ctypes.c_uint64]
         _lib = L
     return _lib
 
@@ -288,6 +293,55 @@ def steady_state(osys, rtol=1e-11, restart=100, maxit=20000, use_ilu=True):
     finally:
         L.orc_csr_free(b)
     return x, its
+
+
+class McwfEnsemble:
+    """Trajectory ensemble of the oracle's MCWF restatement (orc_mcwf):
+    states (ntraj x D), thresholds and draw counters, spawned from psi0 like
+    the engine (threshold = draw 0, counter 1)."""
+
+    def __init__(self, osys, psi0, ntraj, seed):
+        L = lib()
+        self.D = osys.D
+        self.ntraj = ntraj
+        self.seed = seed
+        self.heff = osys.csr_handle(MODE_MCWF)
+        self.jumps, a = [], []
+        for kind, coef, ops in osys.terms:
+            if kind != LINDBLAD or coef == 0:
+                continue
+            one = OSys()
+            one.levels = list(osys.levels)
+            one.ham(1j, *ops)  # -i (i C) = C in the Schroedinger form
+            self.jumps.append(one.csr_handle(MODE_WF))
+            a += [coef.real, coef.imag]
+        self.a = np.array(a if a else [0.0, 0.0], dtype=np.float64)
+        self.psi = np.tile(np.asarray(psi0, dtype=np.complex128), (ntraj, 1)).copy()
+        self.thr = np.array([L.orc_mcwf_draw(seed, i, 0) for i in range(ntraj)], dtype=np.float64)
+        self.cnt = np.ones(ntraj, dtype=np.uint64)
+        self.stats = np.zeros(2 * ntraj, dtype=np.int64)
+
+    def run(self, t0, tmax, dt, scheme=0, atol=5e-7, rtol=5e-7, hmin=0.01, hmax=1.0, max_steps=10 ** 9):
+        L = lib()
+        arr = (ctypes.c_void_p * max(1, len(self.jumps)))(*self.jumps)
+        st = L.orc_mcwf(self.heff, len(self.jumps), ctypes.cast(arr, ctypes.c_void_p), _p(self.a), _p(self.psi),
+                        self.ntraj, _p(self.thr), _p(self.cnt), self.seed, t0, tmax, dt, atol, rtol, hmin, hmax,
+                        scheme, max_steps, _p(self.stats))
+        if st:
+            raise RuntimeError(f"orc_mcwf status {st}")
+
+    def expectation(self, levels, *ops):
+        """Ensemble average of <psi|O|psi>/<psi|psi> (qvec_utilities.c:1353-1424)."""
+        v = 0j
+        for p in self.psi:
+            v += expect_wf(levels, p, *ops) / np.vdot(p, p).real
+        return v / self.ntraj
+
+    def free(self):
+        lib().orc_csr_free(self.heff)
+        for h in self.jumps:
+            lib().orc_csr_free(h)
+        self.jumps = []
 
 
 def num_threads():

@@ -879,3 +879,148 @@ int orc_num_threads(void) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------ MCWF
+ * Quantum-jump trajectories (use_mcwf_solver / _sys_MCWF_PostEventFunction,
+ * qsystem.c:358-403, 1139-1235) with the jump-time location and the random
+ * stream the CUDA engine defines for them: norm threshold r ~ U[0,1), the
+ * crossing of |psi|^2 = r located by bisection on the step length to
+ * 1e-9, jump k with probability Re(a_k) |C_k psi|^2 / total, then
+ * psi <- sqrt(a_k) C_k psi / sqrt(Re(a_k) |C_k psi|^2), new threshold.
+ * Draw k of trajectory i: SplitMix64 (Steele, Lea and Flood, 2014) of
+ * seed ^ SplitMix64((i << 32) ^ k), top 53 bits.  Heff is the mode-2
+ * operator of orc_build, C[k] the jump operators as CSR (one term each),
+ * scheme 0 adaptive BS3 (the orc_bs3 controller), 1 fixed BS3, 2 fixed
+ * classical RK4.  psi (ntraj x D), thr and cnt are advanced in place;
+ * returns 0, or 1 / 2 on a step limit / unlocated jump.                   */
+static uint64_t sm64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+double orc_mcwf_draw(uint64_t seed, i64 i, uint64_t k) {
+  uint64_t h = sm64(seed ^ sm64(((uint64_t)i << 32) ^ k));
+  return (double)(h >> 11) * 0x1.0p-53;
+}
+
+static double mc_norm2(const cplx *x, i64 n) {
+  double s = 0;
+  for (i64 i = 0; i < n; i++) s += creal(x[i]) * creal(x[i]) + cimag(x[i]) * cimag(x[i]);
+  return s;
+}
+
+static double mc_step(const csr *A, int scheme, double atol, double rtol, double h, const cplx *y, cplx *yn,
+                      cplx *k1, cplx *k2, cplx *k3, cplx *k4, cplx *x) {
+  i64 n = A->nrows;
+  orc_spmv(A, (const double *)y, (double *)k1);
+  if (scheme == 2) {
+    for (i64 i = 0; i < n; i++) x[i] = y[i] + 0.5 * h * k1[i];
+    orc_spmv(A, (const double *)x, (double *)k2);
+    for (i64 i = 0; i < n; i++) x[i] = y[i] + 0.5 * h * k2[i];
+    orc_spmv(A, (const double *)x, (double *)k3);
+    for (i64 i = 0; i < n; i++) x[i] = y[i] + h * k3[i];
+    orc_spmv(A, (const double *)x, (double *)k4);
+    for (i64 i = 0; i < n; i++) yn[i] = y[i] + h / 6.0 * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]);
+    return 0.0;
+  }
+  for (i64 i = 0; i < n; i++) x[i] = y[i] + 0.5 * h * k1[i];
+  orc_spmv(A, (const double *)x, (double *)k2);
+  for (i64 i = 0; i < n; i++) x[i] = y[i] + 0.75 * h * k2[i];
+  orc_spmv(A, (const double *)x, (double *)k3);
+  for (i64 i = 0; i < n; i++) yn[i] = y[i] + h * (2.0 / 9.0 * k1[i] + 1.0 / 3.0 * k2[i] + 4.0 / 9.0 * k3[i]);
+  if (scheme != 0) return 0.0;
+  orc_spmv(A, (const double *)yn, (double *)k4);
+  double s = 0;
+  for (i64 i = 0; i < n; i++) {
+    cplx e = h * ((2.0 / 9.0 - 7.0 / 24.0) * k1[i] + (1.0 / 3.0 - 0.25) * k2[i] +
+                  (4.0 / 9.0 - 1.0 / 3.0) * k3[i] - 0.125 * k4[i]);
+    double m = fmax(cabs(y[i]), cabs(yn[i]));
+    double q = cabs(e) / (atol + rtol * m);
+    s += q * q;
+  }
+  return sqrt(s / (double)n);
+}
+
+int orc_mcwf(const csr *Heff, int nJ, const csr *const *C, const double *a, double *psid, int ntraj,
+             double *thr, uint64_t *cnt, uint64_t seed, double t0, double tmax, double dt, double atol,
+             double rtol, double hmin, double hmax, int scheme, i64 max_steps, i64 *stats) {
+  i64 D = Heff->nrows;
+  cplx *y = malloc(D * sizeof(cplx)), *yn = malloc(D * sizeof(cplx)), *k1 = malloc(D * sizeof(cplx)),
+       *k2 = malloc(D * sizeof(cplx)), *k3 = malloc(D * sizeof(cplx)), *k4 = malloc(D * sizeof(cplx)),
+       *x = malloc(D * sizeof(cplx)), *cy = malloc(D * sizeof(cplx));
+  double *pj = malloc((nJ > 0 ? nJ : 1) * sizeof(double));
+  int status = 0;
+  for (int i = 0; i < ntraj && !status; i++) {
+    cplx *psi = (cplx *)psid + (i64)i * D;
+    memcpy(y, psi, D * sizeof(cplx));
+    double r = thr[i];
+    uint64_t c = cnt[i];
+    double t = t0, h = dt;
+    i64 steps = 0, jumps = 0;
+    double tend_tol = 1e-12 * fmax(1.0, fabs(tmax));
+    while (t < tmax - tend_tol) {
+      if (steps >= max_steps) { status = 1; break; }
+      double h_try = h;
+      int last = 0;
+      if (t + h_try >= tmax - tend_tol) { h_try = tmax - t; last = 1; }
+      double err = mc_step(Heff, scheme, atol, rtol, h_try, y, yn, k1, k2, k3, k4, x);
+      double h_next = h;
+      if (scheme == 0) {
+        double fac = err > 0 ? 0.9 * pow(err, -1.0 / 3.0) : 10.0;
+        fac = fmin(10.0, fmax(0.1, fac));
+        h_next = fmin(hmax, fmax(hmin, h_try * fac));
+        if (!(err <= 1.0 || h_try <= hmin * (1 + 1e-12))) { h = h_next; continue; }
+      }
+      if (mc_norm2(yn, D) < r) {
+        double lo = 0.0, hi = h_try, mid = h_try;
+        int found = 0;
+        for (int it = 0; it < 200; it++) {
+          mid = 0.5 * (lo + hi);
+          mc_step(Heff, scheme, atol, rtol, mid, y, yn, k1, k2, k3, k4, x);
+          double nm = mc_norm2(yn, D);
+          if (fabs(nm - r) <= 1e-9) { found = 1; break; }
+          if (nm < r) hi = mid; else lo = mid;
+          if (hi - lo <= 1e-15 * fmax(1.0, fabs(t))) { found = 1; break; }
+        }
+        if (!found) { status = 2; break; }
+        t += mid;
+        double ptot = 0;
+        for (int k = 0; k < nJ; k++) {
+          orc_spmv(C[k], (const double *)yn, (double *)cy);
+          pj[k] = a[2 * k] * mc_norm2(cy, D);
+          ptot += pj[k];
+        }
+        double u = orc_mcwf_draw(seed, i, c++);
+        int kj = -1;
+        double pk = 0, cum = 0;
+        for (int k = 0; k < nJ; k++) {
+          cum += pj[k] / ptot;
+          if (cum >= u) { kj = k; pk = pj[k]; break; }
+        }
+        if (kj >= 0 && pk > 0) {
+          cplx sa = csqrt(a[2 * kj] + I * a[2 * kj + 1]);
+          cplx sc = sa / sqrt(pk);
+          orc_spmv(C[kj], (const double *)yn, (double *)cy);
+          for (i64 q = 0; q < D; q++) y[q] = sc * cy[q];
+          jumps++;
+        } else {
+          double nn = 1.0 / sqrt(mc_norm2(yn, D));
+          for (i64 q = 0; q < D; q++) y[q] = yn[q] * nn;
+        }
+        r = orc_mcwf_draw(seed, i, c++);
+        continue;
+      }
+      memcpy(y, yn, D * sizeof(cplx));
+      steps++;
+      t = last ? tmax : t + h_try;
+      if (scheme == 0) h = h_next;
+    }
+    memcpy(psi, y, D * sizeof(cplx));
+    thr[i] = r;
+    cnt[i] = c;
+    if (stats) { stats[2 * i] += steps; stats[2 * i + 1] += jumps; }
+  }
+  free(y); free(yn); free(k1); free(k2); free(k3); free(k4); free(x); free(cy); free(pj);
+  return status;
+}

@@ -200,6 +200,8 @@ def lib():
         "quac_ensemble_run": (ctypes.c_int, [vp, dbl, dbl, dbl]),
         "quac_ensemble_get_stats": (ctypes.c_int, [vp, i64, P(dbl), P(i64), P(i64), P(ctypes.c_int)]),
         "quac_ensemble_populations": (ctypes.c_int, [vp, vp]),
+        "quac_ensemble_set_redo_margin": (ctypes.c_int, [vp, dbl]),
+        "quac_ensemble_redone_steps": (i64, [vp, i64]),
         "create_op": (None, [ctypes.c_int, P(_OpPtr)]),
         "create_vec": (None, [ctypes.c_int, P(P(_OpPtr))]),
         "add_to_ham": (None, [Scalar, _OpPtr]),
@@ -221,6 +223,9 @@ def lib():
         "get_bitstring_probs": (None, [P(_QvecStruct), P(i64), P(P(dbl)), P(P(dbl))]),
         "quac_add_term_time_dep_list": (ctypes.c_int, [P(_QsysStruct), ctypes.c_int, Scalar, vp, vp, i64,
                                                        P(_OpPtr)]),
+        "use_mcwf_solver": (None, [P(_QsysStruct), i64, i64]),
+        "quac_set_observable_monitor": (ctypes.c_int, [P(_QsysStruct), i64, P(i64), P(_OpPtr), vp, vp, i64]),
+        "quac_mcwf_get_states": (ctypes.c_int, [P(_QvecStruct), vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -799,6 +804,13 @@ class Ensemble:
     def set_options(self, precision=0, atol=5e-7, rtol=5e-7, hmin=0.01, hmax=1.0, max_steps=10 ** 6):
         self._call("quac_ensemble_set_options", precision, atol, rtol, hmin, hmax, max_steps)
 
+    def set_redo_margin(self, margin):
+        """complex64 mode: re-evaluate steps with |err - 1| < margin in complex128."""
+        self._call("quac_ensemble_set_redo_margin", margin)
+
+    def redone_steps(self):
+        return np.array([lib().quac_ensemble_redone_steps(self._h, i) for i in range(self.n)])
+
     def set_shape(self, warps, ctas_per_sm, elems_per_thread):
         self._call("quac_ensemble_set_shape", warps, ctas_per_sm, elems_per_thread)
 
@@ -1048,4 +1060,54 @@ def read_qvec_wf_binary(path):
 
 def print_qvec_file(q, path):
     lib().print_qvec_file(q._ptr, os.fsencode(path))
+    _check()
+
+
+def use_mcwf_solver(qs, num_tot_trajs, seed=0):
+    """Quantum-jump trajectories instead of the density-matrix equations
+    (qsystem.c:358-403); call after the Lindblad terms, before
+    construct_matrix and create_qvec_sys.  seed 0 draws one."""
+    lib().use_mcwf_solver(qs._ptr, int(num_tot_trajs), int(seed))
+    _check()
+
+
+def mcwf_states(q):
+    """(states, stats) of an MCWF ensemble qvec after time_step_sys: states
+    (ntraj, D) unnormalised wavefunctions, stats (ntraj, 2) accepted steps
+    and jumps of every trajectory."""
+    n, D = q._ptr.contents.n_ensemble, q.n
+    st = np.zeros((n, D), dtype=np.complex128)
+    ss = np.zeros((n, 2), dtype=np.int64)
+    lib().quac_mcwf_get_states(q._ptr, st.ctypes.data_as(vp), ss.ctypes.data_as(vp))
+    _check()
+    return st, ss
+
+
+_ObsFn = ctypes.CFUNCTYPE(None, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double),
+                          ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+
+
+def set_observable_monitor(qs, observables, fn, batch=1000):
+    """Records Tr(O rho) (or <psi|O|psi>) of every observable after every
+    step of time_step_sys on the GPU; fn(steps, times, values) receives
+    numpy arrays in batches (values: (n, len(observables)) complex).  Each
+    observable is a tuple of operators (a product).  fn None removes it."""
+    if fn is None:
+        qs._obs_monitor = None
+        lib().quac_set_observable_monitor(qs._ptr, 0, None, None, None, None, 1)
+        _check()
+        return
+    nobs = len(observables)
+
+    def _cb(n, steps, times, vals, ctx):
+        st = np.ctypeslib.as_array(steps, shape=(n,)).copy()
+        tm = np.ctypeslib.as_array(times, shape=(n,)).copy()
+        vv = np.ctypeslib.as_array(vals, shape=(n * nobs * 2,)).copy()
+        fn(st, tm, (vv[0::2] + 1j * vv[1::2]).reshape(n, nobs))
+
+    qs._obs_monitor = _ObsFn(_cb)
+    flat = [o for obs in observables for o in obs]
+    nops = (ctypes.c_int64 * nobs)(*[len(obs) for obs in observables])
+    arr = _oplist(flat)
+    lib().quac_set_observable_monitor(qs._ptr, nobs, nops, arr, ctypes.cast(qs._obs_monitor, vp), None, int(batch))
     _check()

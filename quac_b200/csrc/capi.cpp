@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <random>
 
 #include "runtime.h"
 
@@ -106,7 +107,8 @@ cudaStream_t stream_of(qsystem qs) {
 }
 
 void ensure_program(qsystem qs) {
-  const int mode = qs->dm_equations ? 0 : 1;
+  // 0: density matrix, 1: Schroedinger, 2: MCWF effective Hamiltonian
+  const int mode = qs->mcwf_solver ? 2 : (qs->dm_equations ? 0 : 1);
   if (qs->impl->prog && qs->impl->prog_mode == mode) return;
   if (qs->impl->prog) {
     qs->impl->prog->release();
@@ -139,6 +141,16 @@ static ObsEntry obs_tables(int64_t D, const std::vector<op_handle> &ops) {
   QCUDA(cudaMemcpy(e.val, val.data(), D * sizeof(double2), cudaMemcpyHostToDevice));
   g_obs[key] = e;
   return e;
+}
+
+void ObsMonitor::release() {
+  if (dmap) cudaFree(dmap);
+  if (dval) cudaFree(dval);
+  if (dvalues) cudaFree(dvalues);
+  dmap = nullptr;
+  dval = nullptr;
+  dvalues = nullptr;
+  D = 0;
 }
 
 static void drop_obs_cache_for(op_handle op) {
@@ -267,7 +279,9 @@ void clear_mat_terms_sys(qsystem qs) {
 void destroy_system(qsystem *qsys) {
   qsystem q = *qsys;
   if (!q) return;
+  q->impl->obsmon.release();
   clear_mat_terms_sys(q);
+  mcwf_release_system(q);
   q->impl->ws.release();
   if (q->impl->host_vec) vec_free(q->impl->host_vec);
   if (q->impl->ws.dsum) cudaFree(q->impl->ws.dsum);
@@ -476,8 +490,33 @@ int quac_add_term_time_dep_list(qsystem qs, int kind, PetscScalar a, void *ctx, 
 }
 
 void use_mcwf_solver(qsystem qs, PetscInt num_tot_trajs, PetscInt seed) {
-  (void)qs; (void)num_tot_trajs; (void)seed;
-  fail(9, "ERROR! use_mcwf_solver: the Monte-Carlo wavefunction solver is not provided by this engine\n");
+  if (qs->hspace_frozen) {
+    fail(9, "ERROR! use_mcwf_solver must be called before construct_matrix or create_qvec_sys!\n");
+    return;
+  }
+  if (!qs->dm_equations) {
+    fail(9, "ERROR! use_mcwf_solver must be used with a Lindblad term!\n");
+    return;
+  }
+  if (num_tot_trajs < 2) {
+    fail(9, "ERROR! use_mcwf_solver must be called with more than 2 num_tot_trajs!\n");
+    return;
+  }
+  if (num_tot_trajs > (1 << 30)) { fail(9, "ERROR! num_tot_trajs too large\n"); return; }
+  uint64_t sd = (uint64_t)seed;
+  if (seed == 0) {  // the reference draws a seed (make_sprng_seed) when given NULL
+    std::random_device rd;
+    sd = ((uint64_t)rd() << 32) ^ rd();
+  }
+  qs->hspace_frozen = PETSC_TRUE;
+  qs->mcwf_solver = PETSC_TRUE;
+  qs->impl->mcwf_seed = sd;
+  qs->impl->mcwf_ntraj = num_tot_trajs;
+  if (qs->impl->prog) {
+    qs->impl->prog->release();
+    delete qs->impl->prog;
+    qs->impl->prog = nullptr;
+  }
 }
 
 void construct_matrix(qsystem qs) {
@@ -490,7 +529,8 @@ void construct_matrix(qsystem qs) {
     fail(0, "ERROR! You need to add some terms before you construct\n       a matrix!\n");
     return;
   }
-  qs->dim = qs->dm_equations ? qs->total_levels * qs->total_levels : qs->total_levels;
+  // the MCWF solver works in the wavefunction space (qsystem.c:613-619)
+  qs->dim = (qs->dm_equations && !qs->mcwf_solver) ? qs->total_levels * qs->total_levels : qs->total_levels;
   ensure_program(qs);
   qs->mat_allocated = 1;
 }
@@ -545,8 +585,22 @@ void create_wf_sys(qsystem qs, qvec *out) {
   *out = new_qvec(WAVEFUNCTION, qs->dim, qs->total_levels, qs->num_subsystems, dims.data());
 }
 
+// WF_ENSEMBLE of the MCWF solver (qvec_utilities.c:790-830): data is the
+// initial wavefunction; the trajectories are spawned from it by the first
+// time_step_sys
+static void create_wf_ens_sys(qsystem qs, qvec *out) {
+  qs->dim = qs->total_levels;
+  qs->hspace_frozen = 1;
+  std::vector<PetscInt> dims(qs->num_subsystems);
+  for (PetscInt i = 0; i < qs->num_subsystems; i++) dims[i] = qs->subsystem_list[i]->my_levels;
+  *out = new_qvec(WF_ENSEMBLE, qs->total_levels, qs->total_levels, qs->num_subsystems, dims.data());
+  (*out)->n_ensemble = qs->impl->mcwf_ntraj;
+  (*out)->ens_spawned = PETSC_FALSE;
+}
+
 void create_qvec_sys(qsystem qs, qvec *out) {
-  if (qs->dm_equations) create_dm_sys(qs, out);
+  if (qs->mcwf_solver) create_wf_ens_sys(qs, out);
+  else if (qs->dm_equations) create_dm_sys(qs, out);
   else create_wf_sys(qs, out);
 }
 
@@ -567,6 +621,7 @@ void create_arb_qvec(qvec *out, PetscInt nstates, qvec_type t) {
 
 void destroy_qvec(qvec *q) {
   if (!*q) return;
+  mcwf_release(*q);
   free((*q)->hspace_dims);
   vec_free((*q)->data);
   free(*q);
@@ -636,9 +691,13 @@ void get_expectation_value_qvec_list(qvec q, PetscScalar *val, PetscInt num_ops,
     ObsEntry e = obs_tables(D, v);
     cplx r = dm_expectation(q->data->d, D, e.map, e.val, g_default_stream());
     *val = PetscScalar(r.real(), r.imag());
-  } else if (q->my_type == WAVEFUNCTION) {
+  } else if (q->my_type == WAVEFUNCTION || (q->my_type == WF_ENSEMBLE && !mcwf_spawned(q))) {
     ObsEntry e = obs_tables(q->n, v);
     cplx r = wf_expectation(q->data->d, q->n, e.map, e.val, g_default_stream());
+    *val = PetscScalar(r.real(), r.imag());
+  } else if (q->my_type == WF_ENSEMBLE) {
+    ObsEntry e = obs_tables(q->n, v);
+    cplx r = mcwf_expectation(q, e.map, e.val);
     *val = PetscScalar(r.real(), r.imag());
   } else {
     fail(0, "ERROR! qvec type not understood.");
@@ -1173,6 +1232,63 @@ void steady_state(Vec x) {
   free(tmp);
   if (its >= 0) printf("Iterations %ld\n", (long)its);
 }
+
+int quac_set_observable_monitor(qsystem qs, PetscInt nobs, const PetscInt *nops, op_handle *ops,
+                                quac_observable_monitor cb, void *ctx, PetscInt batch) {
+  ObsMonitor &M = qs->impl->obsmon;
+  M.release();
+  M.obs.clear();
+  M.cb = cb;
+  M.ctx = ctx;
+  if (!cb) return 0;
+  if (nobs < 1 || nobs > 64 || batch < 1 || batch > (1 << 20)) {
+    fail(0, "ERROR! observable monitor: 1..64 observables and a batch of 1..2^20 steps\n");
+    M.cb = nullptr;
+    return 1;
+  }
+  PetscInt k = 0;
+  for (PetscInt o = 0; o < nobs; o++) {
+    if (nops[o] < 1) { fail(0, "ERROR! observable %ld has no operators\n", (long)o); M.cb = nullptr; return 1; }
+    std::vector<op_handle> v(ops + k, ops + k + nops[o]);
+    for (op_handle h : v)
+      if (!h) { fail(9, "ERROR! NULL operator in an observable\n"); M.cb = nullptr; return 1; }
+    M.obs.push_back(v);
+    k += nops[o];
+  }
+  M.batch = batch;
+  return 0;
+}
+
+}  // extern "C"
+
+namespace quac {
+// Device tables of the monitor's observables for dimension D
+void observable_monitor_tables(qsystem qs, int64_t D) {
+  ObsMonitor &M = qs->impl->obsmon;
+  if (M.D == D && M.dmap) return;
+  M.release();
+  const int nobs = (int)M.obs.size();
+  std::vector<int> maps;
+  std::vector<double2> vals;
+  std::vector<int> map;
+  std::vector<cplx> val;
+  for (auto &ops : M.obs) {
+    op_chain_map(D, ops, map, val);
+    for (int64_t r = 0; r < D; r++) {
+      maps.push_back(map[r]);
+      vals.push_back(make_double2(val[r].real(), val[r].imag()));
+    }
+  }
+  QCUDA(cudaMalloc(&M.dmap, maps.size() * sizeof(int)));
+  QCUDA(cudaMalloc(&M.dval, vals.size() * sizeof(double2)));
+  QCUDA(cudaMalloc(&M.dvalues, (size_t)M.batch * nobs * sizeof(double2)));
+  QCUDA(cudaMemcpy(M.dmap, maps.data(), maps.size() * sizeof(int), cudaMemcpyHostToDevice));
+  QCUDA(cudaMemcpy(M.dval, vals.data(), vals.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  M.D = D;
+}
+}  // namespace quac
+
+extern "C" {
 
 // legacy density-matrix helpers (dm_utilities.c): the Vec holds the
 // column-stacked density matrix of the legacy system

@@ -175,7 +175,8 @@ struct DeviceProgram {
 };
 
 // Builds the device program of a qsystem's time-independent terms.
-// mode 0 = density matrix (L on D^2), 1 = Schroedinger (-iH on D).
+// mode 0 = density matrix (L on D^2), 1 = Schroedinger (-iH on D),
+// 2 = MCWF effective Hamiltonian (-i H_eff on D).
 DeviceProgram *compile_terms(qsystem qs, int mode);
 
 // Kernel launchers (lrho.cu, lrho_qubit.cu)

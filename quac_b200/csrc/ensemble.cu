@@ -80,8 +80,8 @@ struct EnsItem {
 struct EnsStatus {
   double t, h;
   long long steps, rejected;
-  int flags;  // 1: step limit reached, 2: non-finite error norm
-  int pad;
+  int flags;   // 1: step limit reached, 2: non-finite error norm
+  int redone;  // complex64 mode: steps whose estimate was taken again in complex128
 };
 
 struct EnsParams {
@@ -98,6 +98,7 @@ struct EnsParams {
   int *counter;
   double t0, tmax, h0, atol, rtol, hmin, hmax;
   long long max_steps;
+  double redo_margin;    // complex64 mode: |err - 1| below this re-evaluates the step in complex128
 };
 
 __device__ __forceinline__ void cmac(double &ax, double &ay, double2 a, double2 b) {
@@ -261,7 +262,7 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
   float2 *const Kb32 = (float2 *)Kb64;                      // dK_{j+2} at Kb32 + j C
   int iy = 0;
   double t = P.t0, h = P.h0;
-  long long steps = 0, rej = 0;
+  long long steps = 0, rej = 0, redo = 0;
   int flags = 0;
   const double tend_tol = 1e-12 * fmax(1.0, fabs(P.tmax));
   double bsum = 0.0;
@@ -284,16 +285,12 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
   eval64_into(K1);
   group_sync(gi, gw);
 
-  while (t < P.tmax - tend_tol) {
-    if (steps >= P.max_steps) { flags |= 1; break; }
-    bool last = false;
-    double ht = h;
-    if (t + ht >= P.tmax - tend_tol) { ht = P.tmax - t; last = true; }
-    const double2 *y = iy ? yb : ys;
-    double2 *y5 = iy ? ys : yb;
-    // stages 2..6
+  // one attempt of the step from (t, y) with length ht: stages 2..7 into
+  // the slot, y5, and the weighted error norm; f64 = all stages complex128
+  // (MODE 0, and MODE 1's re-evaluation near the accept threshold)
+  auto attempt = [&](bool f64, double ht, const double2 *y, double2 *y5) -> double {
     for (int s = 1; s < 6; s++) {
-      if (MODE == 0) {
+      if (f64) {
         for_rounds<U>(lt, gt, D, [&](const int(&e)[U], const int(&)[U], const int(&)[U], const bool(&ok)[U]) {
 #pragma unroll
           for (int u = 0; u < U; u++) {
@@ -317,7 +314,7 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
         });
       }
       group_sync(gi, gw);
-      if (MODE == 0) {
+      if (f64) {
         eval64_into(Kb64 + (size_t)(s - 1) * C);
       } else {
         float2 *dst = Kb32 + (size_t)(s - 1) * C;
@@ -337,7 +334,7 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
       for (int u = 0; u < U; u++) {
         if (!ok[u]) continue;
         double2 v;
-        if (MODE == 0) {
+        if (f64) {
           v = axpy(y[e[u]], ht * eA[6][0], K1[e[u]]);
           for (int j = 1; j < 6; j++) v = axpy(v, ht * eA[6][j], Kb64[(size_t)(j - 1) * C + e[u]]);
         } else {
@@ -354,7 +351,7 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
     double loc = 0.0;
     for (ElemIt it(lt, gt, D); it.ok(); it.next()) {
       double2 er;
-      if (MODE == 0) {
+      if (f64) {
         er = axpy(make_double2(0.0, 0.0), ht * eE[0], K1[it.e]);
         for (int j = 1; j < 6; j++) er = axpy(er, ht * eE[j], Kb64[(size_t)(j - 1) * C + it.e]);
         er = axpy(er, ht * eE[6], K7[it.e]);
@@ -369,7 +366,24 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
       const double q = sqrt(er.x * er.x + er.y * er.y) / (P.atol + P.rtol * m);
       loc += q * q;
     }
-    const double err = sqrt(group_sum(loc, gi, gw, red) / (double)n);
+    return sqrt(group_sum(loc, gi, gw, red) / (double)n);
+  };
+
+  while (t < P.tmax - tend_tol) {
+    if (steps >= P.max_steps) { flags |= 1; break; }
+    bool last = false;
+    double ht = h;
+    if (t + ht >= P.tmax - tend_tol) { ht = P.tmax - t; last = true; }
+    const double2 *y = iy ? yb : ys;
+    double2 *y5 = iy ? ys : yb;
+    double err = attempt(MODE == 0, ht, y, y5);
+    // MODE 1: an estimate near the accept threshold is taken again with
+    // complex128 stages, so accept / reject follows the complex128 decision
+    if (MODE == 1 && isfinite(err) && fabs(err - 1.0) < P.redo_margin) {
+      group_sync(gi, gw);
+      err = attempt(true, ht, y, y5);
+      redo++;
+    }
     if (!isfinite(err)) { flags |= 2; break; }
     double fac = err > 0 ? 0.9 * pow(err, -0.2) : 10.0;
     fac = fmin(10.0, fmax(0.1, fac));
@@ -397,7 +411,7 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
     st.steps = steps;
     st.rejected = rej;
     st.flags = flags;
-    st.pad = 0;
+    st.redone = (int)redo;
     P.status[I.id] = st;
   }
 }
@@ -455,6 +469,7 @@ struct quac_ensemble_s {
   int mode = 0;
   double atol = 5e-7, rtol = 5e-7, hmin = 0.01, hmax = 1.0;
   long long max_steps = 1000000;
+  double redo_margin = 0.5;
   int warps = 16, cps = 1, ept = 8;  // launch shape
   // device
   unsigned char *d_tables = nullptr, *d_scratch = nullptr;
@@ -558,7 +573,9 @@ bool build_plan(quac_ensemble E) {
   std::vector<EnsItem> sorted(items.size());
   for (size_t k = 0; k < io.size(); k++) sorted[k] = items[io[k]];
   slot_elems = (slot_elems + 1) / 2 * 2;
-  const long long bpe = (E->mode == 0) ? 8 * 16 : 3 * 16 + 5 * 8;
+  // complex128 stage storage in both modes: the complex64 mode re-evaluates
+  // steps near the accept threshold with complex128 stages
+  const long long bpe = 8 * 16;
   const int grid = num_sms_ens() * E->cps;
   const size_t need = (size_t)grid * E->warps * slot_elems * bpe;
   if (need > E->scratch_bytes) {
@@ -594,6 +611,7 @@ bool build_plan(quac_ensemble E) {
   p.hmin = E->hmin;
   p.hmax = E->hmax;
   p.max_steps = E->max_steps;
+  p.redo_margin = E->redo_margin;
   E->grid = grid;
   E->smem = (size_t)arena * E->warps;
   E->plan_valid = true;
@@ -785,6 +803,19 @@ int quac_ensemble_set_options(quac_ensemble E, int precision, double atol, doubl
   E->max_steps = max_steps;
   E->plan_valid = false;
   return 0;
+}
+
+int quac_ensemble_set_redo_margin(quac_ensemble E, double margin) {
+  if (!(margin >= 0.0) || margin > 1.0) { fail(0, "ERROR! ensemble redo margin must lie in [0, 1]\n"); return 1; }
+  E->redo_margin = margin;
+  E->plan_valid = false;
+  return 0;
+}
+
+int64_t quac_ensemble_redone_steps(quac_ensemble E, int64_t i) {
+  if (i < 0 || i >= E->n) { fail(0, "ERROR! ensemble index out of range\n"); return -1; }
+  if (!read_status(E)) return -1;
+  return E->status[i].redone;
 }
 
 int quac_ensemble_set_shape(quac_ensemble E, int warps, int ctas_per_sm, int elems_per_thread) {

@@ -187,6 +187,7 @@ struct Stepper {
 // Runs the integration on vector v (device-resident, length qs->dim).  The
 // qvec (if any) receives circuit gates and is handed to the monitor.
 int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int64_t steps_max) {
+  if (qs->mcwf_solver) return mcwf_integrate(qs, x, t0, tmax, dt, steps_max);
   ensure_program(qs);
   if (has_error() || !qs->impl->prog) return 1;
   const DeviceProgram &PP = *qs->impl->prog;
@@ -218,6 +219,52 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
   if (o.herm_mode && !td && PP.herm_ok && PP.has_qubit && !PP.passes.empty() && P.ncols == P.D && events.empty())
     herm = hermitian_asymmetry(v->d, P.D, s) <= 1e-13 ? 1 : 0;
   Stepper st{qs, &PP, s, n, o.atol, o.rtol, herm};
+  ObsMonitor &OM = qs->impl->obsmon;
+  const int nobs = OM.cb ? (int)OM.obs.size() : 0;
+  if (nobs) observable_monitor_tables(qs, P.D);
+  if (has_error()) return 1;
+  // monitored small system, fixed RK4, nothing else per step: many steps
+  // per launch with the state in shared memory (small_run.cu)
+  if (nobs && !qs->ts_monitor && fixed && rk4 && !o.rk4_classic && !td && events.empty() && P.ncols == P.D &&
+      small_rk4_eligible(PP)) {
+    const double tol = 1e-12 * std::max(1.0, std::fabs(tmax));
+    std::vector<double> hs, ts;
+    double tt = t0;
+    while ((int64_t)hs.size() < steps_max && tt < tmax - tol) {
+      double h_try = dt;
+      bool last = false;
+      if (tt + h_try >= tmax - tol) { h_try = tmax - tt; last = true; }
+      hs.push_back(h_try);
+      tt = last ? tmax : tt + h_try;
+      ts.push_back(tt);
+    }
+    std::vector<PetscScalar> vals;
+    std::vector<PetscInt> stepno;
+    for (size_t i = 0; i < hs.size() && !has_error();) {
+      size_t j = i;
+      while (j < hs.size() && (int64_t)(j - i) < OM.batch && hs[j] == hs[i]) j++;
+      const int cnt = (int)(j - i);
+      launch_small_rk4(PP, v->d, cnt, hs[i], nobs, OM.dmap, OM.dval, OM.dvalues, s);
+      vals.resize((size_t)cnt * nobs);
+      QCUDA(cudaMemcpyAsync(vals.data(), OM.dvalues, vals.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+      QCUDA(cudaStreamSynchronize(s));
+      stepno.resize(cnt);
+      for (int k = 0; k < cnt; k++) stepno[k] = (PetscInt)(i + k + 1);
+      OM.cb(cnt, stepno.data(), ts.data() + i, vals.data(), OM.ctx);
+      i = j;
+    }
+    qs->current_time = hs.empty() ? t0 : ts.back();
+    return has_error() ? 1 : 0;
+  }
+  std::vector<PetscInt> ob_steps;
+  std::vector<PetscReal> ob_times;
+  std::vector<PetscScalar> ob_vals;
+  auto flush_obs = [&]() {
+    if (!ob_steps.empty()) OM.cb((PetscInt)ob_steps.size(), ob_steps.data(), ob_times.data(), ob_vals.data(), OM.ctx);
+    ob_steps.clear();
+    ob_times.clear();
+    ob_vals.clear();
+  };
   size_t next_ev = 0;
   _p_TS ts;
   ts.t = t0;
@@ -346,7 +393,19 @@ int integrate(qsystem qs, qvec x, Vec v, double t0, double tmax, double dt, int6
       ts.step = steps;
       qs->ts_monitor(&ts, steps, t, v, qs->ts_ctx);
     }
+    if (nobs) {
+      for (int ob = 0; ob < nobs; ob++) {
+        const int *m = OM.dmap + (size_t)ob * P.D;
+        const double2 *w = OM.dval + (size_t)ob * P.D;
+        const cplx e = P.ncols == P.D ? dm_expectation(v->d, P.D, m, w, s) : wf_expectation(v->d, P.D, m, w, s);
+        ob_vals.push_back(PetscScalar(e.real(), e.imag()));
+      }
+      ob_steps.push_back(steps);
+      ob_times.push_back(t);
+      if ((int64_t)ob_steps.size() >= OM.batch) flush_obs();
+    }
   }
+  if (nobs) flush_obs();
   // one wait at the end: the error-flag read-back is queued behind the last
   // stage (check_program_error synchronises), or a plain stream sync
   if (qs->impl->prog->errflag) check_program_error(*qs->impl->prog, s);

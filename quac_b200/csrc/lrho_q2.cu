@@ -20,6 +20,7 @@
 // serves both, halving that pass's reads of x.
 #include <algorithm>
 #include <array>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <atomic>
@@ -726,20 +727,20 @@ void launch_pass(const PassParams &pp, const CUtensorMap &map, const CUtensorMap
   k_qpass<REAL, TMA, CANON, F32><<<grid, QT, smem, s>>>(pp, map, bmap, x, e);
 }
 
-template <bool F32>
+template <bool TMA, bool F32>
 struct Canon {
   template <int CANON>
   static void launch(const PassParams &pp, const CUtensorMap &map, const CUtensorMap &bmap, const double2 *x,
                      const Epi &e, int grid, size_t smem, cudaStream_t s, bool dry) {
-    launch_pass<true, true, CANON, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
+    launch_pass<true, TMA, CANON, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
   }
 };
 
-// canonical fast path: real mode, TMA, no general terms in this pass
-template <bool F32>
+// canonical fast path: real mode, no general terms in this pass
+template <bool TMA, bool F32>
 void launch_canon_mask(int mask, const PassParams &pp, const CUtensorMap &map, const CUtensorMap &bmap,
                        const double2 *x, const Epi &e, int grid, size_t smem, cudaStream_t s, bool dry) {
-#define launch_canon Canon<F32>::template launch
+#define launch_canon Canon<TMA, F32>::template launch
   switch (mask) {
     case 0: launch_canon<0>(pp, map, bmap, x, e, grid, smem, s, dry); break;
     case 1: launch_canon<1>(pp, map, bmap, x, e, grid, smem, s, dry); break;
@@ -776,9 +777,9 @@ template <bool F32>
 void launch_any_pass(const PassParams &pp, const CUtensorMap &map, const CUtensorMap &bmap, const double2 *x,
                      const Epi &e, int grid, size_t smem, cudaStream_t s, bool dry) {
   const bool tma = pp.tma != 0;
-  const bool only_canon = pp.real && tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 &&
-                          pp.nspill == 0;
-  if (only_canon) launch_canon_mask<F32>(canon_mask(pp), pp, map, bmap, x, e, grid, smem, s, dry);
+  const bool only_canon = pp.real && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 && pp.nspill == 0;
+  if (only_canon && tma) launch_canon_mask<true, F32>(canon_mask(pp), pp, map, bmap, x, e, grid, smem, s, dry);
+  else if (only_canon) launch_canon_mask<false, F32>(canon_mask(pp), pp, map, bmap, x, e, grid, smem, s, dry);
   else if (pp.real && tma) launch_pass<true, true, -1, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
   else if (pp.real) launch_pass<true, false, -1, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
   else if (tma) launch_pass<false, true, -1, F32>(pp, map, bmap, x, e, grid, smem, s, dry);
@@ -790,8 +791,7 @@ void launch_any_pass(const PassParams &pp, const CUtensorMap &map, const CUtenso
 // coefficients, real jumps): its tile (b, a) result is the conjugate
 // transpose of its tile (a, b) result.
 bool hermitian_canonical_pass(const PassParams &pp) {
-  if (!(pp.real && pp.tma && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 && pp.nspill == 0 &&
-        !pp.diag))
+  if (!(pp.real && pp.nL == 0 && pp.nR == 0 && pp.nJ == 0 && pp.nJx == 0 && pp.nspill == 0 && !pp.diag))
     return false;
   for (int b = 0; b < 6; b++)
     if (pp.hl[b] != -pp.hr[b]) return false;

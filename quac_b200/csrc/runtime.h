@@ -30,6 +30,18 @@ struct Term {
 };
 
 struct DeviceProgram;
+// Observables recorded on the device every step (quac_set_observable_monitor)
+struct ObsMonitor {
+  std::vector<std::vector<op_handle>> obs;
+  quac_observable_monitor cb = nullptr;
+  void *ctx = nullptr;
+  int64_t batch = 1000;
+  int *dmap = nullptr;        // nobs x D observable row maps (device)
+  double2 *dval = nullptr;    // nobs x D values
+  double2 *dvalues = nullptr; // batch x nobs recorded values
+  int64_t D = 0;
+  void release();
+};
 // A time-dependent term: its superoperator with coefficient 1, scaled by
 // a f(t) at every stage (qsystem.c:1300-1330)
 struct TdTerm {
@@ -80,6 +92,9 @@ struct qsystem_impl {
   std::vector<op_handle> owned_ops;  // every operator struct created for this system
   Vec host_vec = nullptr;            // device state of quac_time_step_host, kept between calls
   std::vector<quac::TdTerm> td;      // time-dependent terms
+  quac::ObsMonitor obsmon;           // quac_set_observable_monitor
+  uint64_t mcwf_seed = 0;            // use_mcwf_solver
+  int64_t mcwf_ntraj = 0;
   double2 *td_acc = nullptr;         // L(t) x and one term's contribution (2 x dim, lazily allocated)
   int64_t td_acc_n = 0;
 };
@@ -92,6 +107,18 @@ void ensure_program(qsystem qs);
 // term group by term group and the epilogue runs as its own pass
 void apply_L(qsystem qs, double t, const double2 *x, const Epi &e, cudaStream_t s);
 void release_td_programs(qsystem qs);
+// MCWF trajectories (mcwf.cu)
+int mcwf_integrate(qsystem qs, qvec x, double t0, double tmax, double dt, int64_t steps_max);
+bool mcwf_spawned(qvec q);
+void mcwf_release(qvec q);
+void mcwf_release_system(qsystem qs);
+cplx mcwf_expectation(qvec q, const int *map, const double2 *val);
+// device tables of the observable monitor's observables (capi.cpp)
+void observable_monitor_tables(qsystem qs, int64_t D);
+// small_run.cu
+bool small_rk4_eligible(const DeviceProgram &P);
+void launch_small_rk4(const DeviceProgram &P, double2 *state, int nsteps, double h, int nobs, const int *omap,
+                      const double2 *oval, double2 *values, cudaStream_t s);
 int64_t vec_len(Vec v);
 void vec_sync_to_device(Vec v);       // flush pending host additions
 Vec vec_new(int64_t n);

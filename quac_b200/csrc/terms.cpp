@@ -210,10 +210,17 @@ bool compile_host(qsystem qs, int mode, HostProg &hp) {
         }
       }
     } else {
-      if (mode != 0) fail(0, "ERROR! Lindblad terms need the density-matrix equations\n");
+      if (mode == 1) fail(0, "ERROR! Lindblad terms need the density-matrix equations\n");
       std::vector<double> gam(D, 0.0);
       for (int64_t r = 0; r < D; r++)
         if (map[r] >= 0) gam[map[r]] += std::norm(val[r]);
+      if (mode == 2) {
+        // MCWF effective Hamiltonian H - i/2 sum a C^dag C (kron.c:664-700),
+        // applied as -i H_eff: C^dag C is diagonal (C has at most one
+        // nonzero per row and column), so the term adds -a/2 |C|^2 to dr
+        for (int64_t r = 0; r < D; r++) hp.dr[r] += -0.5 * t.a * gam[r];
+        continue;
+      }
       for (int64_t r = 0; r < D; r++) {
         hp.dr[r] += -0.5 * t.a * gam[r];
         hp.dc[r] += -0.5 * t.a * gam[r];

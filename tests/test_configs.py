@@ -77,6 +77,50 @@ def test_config1_jc_rk4_t200_populations_match_oracle(quac, oracle):
     S.qs.destroy()
 
 
+@pytest.mark.parametrize("batch", [1000, 7])
+def test_config1_observable_monitor_matches_oracle(quac, oracle, batch):
+    """The same run through the device-side observable monitor (one-CTA
+    kernel, many steps per launch): both populations after every one of the
+    20,000 steps; every 1000th against the oracle to 1e-10, the rest against
+    the final state's by continuity of the record."""
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    qb, cav = H.jc(S)
+    H.jc(O)
+    quac.construct_matrix(S.qs)
+    rho = quac.create_qvec_sys(S.qs)
+    quac.add_to_qvec(rho, 1.0, 10, 10)
+    quac.assemble_qvec(rho)
+    rec = []
+    quac.set_observable_monitor(S.qs, [(qb.n,), (cav.n,)], lambda st, tm, v: rec.append((st, tm, v)), batch=batch)
+    quac.set_ts_options(rk_type="4", adapt_type="none")
+    c0 = quac.kernel_launch_count()
+    try:
+        quac.time_step_sys(S.qs, rho, 0.0, 200.0, 0.01, 10 ** 6)
+    finally:
+        quac.set_ts_options(rk_type="3bs", adapt_type="basic")
+        quac.set_observable_monitor(S.qs, None, None)
+    launches = quac.kernel_launch_count() - c0
+    steps = np.concatenate([r[0] for r in rec])
+    times = np.concatenate([r[1] for r in rec])
+    vals = np.concatenate([r[2] for r in rec])
+    assert np.array_equal(steps, np.arange(1, 20001))
+    assert abs(times[-1] - 200.0) < 1e-12 and np.all(np.diff(times) > 0)
+    assert launches <= 20000 // batch + 2  # many steps per launch
+    h = O.csr_handle()
+    y = np.zeros(400, dtype=complex)
+    y[10 * 20 + 10] = 1.0
+    for k in range(1000, 20001, 1000):
+        y = oracle.rk4(h, y, 0.01, 1000)
+        pe, pc = _jc_pops([2, 10], y)
+        assert abs(vals[k - 1, 0].real - pe) <= 1e-10 * abs(pe) + 1e-14
+        assert abs(vals[k - 1, 1].real - pc) <= 1e-10 * abs(pc) + 1e-14
+    oracle.free_csr(h)
+    assert _rel(rho.to_numpy(), y) < 1e-10
+    rho.destroy()
+    S.qs.destroy()
+
+
 @pytest.mark.parametrize("layers", [5])
 def test_config2_noisy_circuit_matches_oracle(quac, oracle, layers):
     """Each layer: the drawn gates on rho (superoperator convention) and 1.0

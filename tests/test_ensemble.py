@@ -117,6 +117,31 @@ def test_ensemble_fp32_rhs_population_error(quac, reference):
     E.destroy()
 
 
+@pytest.mark.parametrize("tol", [1e-10])
+def test_ensemble_fp32_rhs_within_1e8_of_oracle_at_tight_tolerance(quac, oracle, tol):
+    """complex64 right-hand-side increments with the steps near the accept
+    threshold re-evaluated in complex128, at a tolerance where the
+    integration error itself is below the bar: every instance's populations
+    within 1e-8 of the oracle's complex128 DP5 at the same tolerance."""
+    params = Sy.driven_jc_ensemble_params(64, seed=11, nc_lo=5, nc_hi=40)
+    E, rho0 = _ensemble(quac, params)
+    E.set_options(precision=1, atol=tol, rtol=tol)
+    E.set_states(rho0)
+    E.run(0.0, T_END, DT0)
+    y = E.get_states()
+    assert E.redone_steps().sum() > 0
+    ref = _oracle_states(oracle, params, T_END, atol=tol, rtol=tol)
+    worst = 0.0
+    for i, (yo, _, _) in enumerate(ref):
+        D = E.dims[i]
+        yi = y[E.offsets[i]:E.offsets[i + 1]].reshape(D, D, order="F")
+        ro = yo.reshape(D, D, order="F")
+        worst = max(worst, np.abs(yi.diagonal().real - ro.diagonal().real).max())
+    print(f"fp32-rhs worst population error at tol {tol:g}: {worst:.3e}")
+    assert worst <= 1e-8
+    E.destroy()
+
+
 def test_ensemble_rejects_bad_input(quac):
     E, rho0 = _ensemble(quac, PARAMS[:2])
     with pytest.raises(quac.QuacError):

@@ -141,8 +141,63 @@ def cpu_baseline(seconds=12.0, rows_frac=64):
     O.free_csr(h)
     gbs = n * nrows * 32 / dt / 1e9
     return {"value": gbs, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
+            "omp_threads": O.num_threads(), "mpi_ranks": 1,
             "sample": f"CSR SpMV over rows [0, D^2/{rows_frac}) of the D=4096 Liouvillian "
                       f"({nrows} rows), {n} applications in {dt:.1f} s, OpenMP"}
+
+
+def cpu_baselines_other_configs(seconds_each=8.0):
+    """The oracle's CPU restatement of the reference algorithm (assembled
+    CSR, one SpMV per stage, OpenMP) on bounded samples of configs 1, 2
+    and 4, in the units of their GPU sections."""
+    from oracle import oracle as O
+    from quac_b200 import systems as Sy
+    out = {"omp_threads": O.num_threads(), "mpi_ranks": 1}
+    # config 1: JC 2 x 10, fixed RK4 dt = 0.01 (no per-step observables on the CPU side)
+    S = O.OSys()
+    Sy.jc(S)
+    h = S.csr_handle()
+    y = np.zeros(400, dtype=complex)
+    y[10 * 20 + 10] = 1.0
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds_each:
+        y = O.rk4(h, y, 0.01, 1000)
+        n += 1000
+    O.free_csr(h)
+    out["jc_rk4_steps_per_s"] = n / (time.perf_counter() - t0)
+    # config 2: noisy 10-qubit circuit, gates (superoperator form) + 1.0 time unit of BS3 per layer
+    S = O.OSys()
+    Sy.noisy_qubits(S, 10)
+    h = S.csr_handle()
+    spec = Sy.noisy_circuit_layers(10, 40)
+    y = np.zeros(1024 * 1024, dtype=complex)
+    y[0] = 1.0
+    n, t, t0 = 0, 0.0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds_each and n < len(spec):
+        for g, qb, kw in spec[n]:
+            y = O.gate_superop([2] * 10, y, g, list(qb), **kw)
+        y, _, _ = O.bs3(h, y, t, t + 1.0, 0.1)
+        t += 1.0
+        n += 1
+    O.free_csr(h)
+    out["circuit_layers_per_s"] = n / (time.perf_counter() - t0)
+    # config 4: driven JC instances one at a time, DP5 atol = rtol = 5e-7 to t = 100
+    params = Sy.driven_jc_ensemble_params(4096)
+    rng = np.random.default_rng(1)
+    n, t0 = 0, time.perf_counter()
+    for i in rng.permutation(4096):
+        if time.perf_counter() - t0 >= seconds_each:
+            break
+        p = params[i]
+        S = O.OSys()
+        Sy.driven_jc(S, **p)
+        h = S.csr_handle()
+        O.dp5(h, Sy.excited_vacuum(p["nc"]), 0.0, 100.0, 0.05)
+        O.free_csr(h)
+        n += 1
+    out["ensemble_solves_per_s"] = n / (time.perf_counter() - t0)
+    out["samples"] = "JC: RK4 steps for ~8 s; circuit: layers for ~8 s; ensemble: random instances for ~8 s"
+    return out
 
 
 def run_reference(args, rank, world):
@@ -178,7 +233,7 @@ def run_reference(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic", "config": workload_config(args.gpus),
         "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
-                         "sample": sample},
+                         "omp_threads": O.num_threads(), "mpi_ranks": 1, "sample": sample},
         "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference PETSc build unavailable (PETSc/SLEPc absent); oracle port of the "
                 "reference algorithm timed instead"}))
@@ -506,6 +561,8 @@ def run_ours(args, rank, world, local_rank):
         out["jc"] = jc_summary(q)
         out["circuit"] = circuit_summary(q)
         out["steady_state"] = steady_summary(q)
+        if not args.no_cpu_baseline:
+            out["cpu_baseline_other_configs"] = cpu_baselines_other_configs()
     q.set_ts_options(rk_type="3bs", adapt_type="basic")
     rho.destroy()
     qs.destroy()

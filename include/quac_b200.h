@@ -234,6 +234,20 @@ void schedule_circuit_layers(qsystem qsys, circuit *circ);            /* quantum
 void apply_circuit_to_sys(qsystem qsys, circuit *circ, PetscReal time); /* quantum_circuits.c:407-431 */
 void apply_circuit_to_qvec(qsystem qsys, circuit circ, qvec q);       /* quantum_circuits.c:143-159 */
 void apply_gate2(qvec q, gate_type g, ...);             /* quantum_circuits.c:776-847 */
+/* Non-variadic form of add_gate_to_circuit_sys for bindings (no reference
+ * counterpart): nq qubits, angles theta / phi / lambda, CUSTOM gates take
+ * ctx and func.  Returns 0 on success. */
+int quac_add_gate(circuit *circ, double time, int gate, int nq, const int *qubits, double theta, double phi,
+                  double lambda, void *ctx, void *func);
+
+/* ------------------------------------------------ circuit front ends */
+/* qasm_parser.h: each reads a file into a new circuit (one gate per
+ * instruction) and sets *num_qubits. */
+void qiskit_qasm_read(char filename[], PetscInt *num_qubits, circuit *circ);  /* qasm_parser.c:583-650 */
+void qiskit_tqasm_read(char filename[], PetscInt *num_qubits, circuit *circ); /* qasm_parser.c:652-718 */
+void cirq_qasm_read(char filename[], PetscInt *num_qubits, circuit *circ);    /* qasm_parser.c:720-787 */
+void projectq_qasm_read(char filename[], PetscInt *num_qubits, circuit *circ); /* qasm_parser.c:195-258 */
+void quil_read(char filename[], PetscInt *num_qubits, circuit *circ);         /* qasm_parser.c:12-72 */
 
 /* ------------------------------------------------- legacy global API */
 void create_op(int levels, op_handle *op);              /* operators.c:59-200 */

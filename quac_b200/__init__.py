@@ -225,6 +225,11 @@ def lib():
                                                        P(_OpPtr)]),
         "use_mcwf_solver": (None, [P(_QsysStruct), i64, i64]),
         "quac_set_observable_monitor": (ctypes.c_int, [P(_QsysStruct), i64, P(i64), P(_OpPtr), vp, vp, i64]),
+        "qiskit_qasm_read": (None, [ctypes.c_char_p, P(i64), P(_CircuitStruct)]),
+        "qiskit_tqasm_read": (None, [ctypes.c_char_p, P(i64), P(_CircuitStruct)]),
+        "cirq_qasm_read": (None, [ctypes.c_char_p, P(i64), P(_CircuitStruct)]),
+        "projectq_qasm_read": (None, [ctypes.c_char_p, P(i64), P(_CircuitStruct)]),
+        "quil_read": (None, [ctypes.c_char_p, P(i64), P(_CircuitStruct)]),
         "quac_mcwf_get_states": (ctypes.c_int, [P(_QvecStruct), vp, vp]),
     }
     for name, (res, args) in sig.items():
@@ -629,6 +634,47 @@ class Circuit:
 
 def create_circuit(num_gates):
     return Circuit(num_gates)
+
+
+def _read_circuit(fn_name, path):
+    c = Circuit.__new__(Circuit)
+    c.c = _CircuitStruct()
+    c._ctx = []
+    nq = ctypes.c_int64()
+    getattr(lib(), fn_name)(os.fsencode(path), ctypes.byref(nq), ctypes.byref(c.c))
+    _check()
+    return nq.value, c
+
+
+def qiskit_qasm_read(path):
+    """(num_qubits, Circuit) from an OpenQASM 2 file in qiskit's qubit order."""
+    return _read_circuit("qiskit_qasm_read", path)
+
+
+def qiskit_tqasm_read(path):
+    return _read_circuit("qiskit_tqasm_read", path)
+
+
+def cirq_qasm_read(path):
+    return _read_circuit("cirq_qasm_read", path)
+
+
+def projectq_qasm_read(path):
+    return _read_circuit("projectq_qasm_read", path)
+
+
+def quil_read(path):
+    return _read_circuit("quil_read", path)
+
+
+def circuit_gates(c):
+    """The gate list of a Circuit as (time, gate type, qubits, theta, phi, lambda) tuples."""
+    out = []
+    for k in range(c.c.num_gates):
+        g = c.c.gate_list[k]
+        out.append((g.time, g.my_gate_type, tuple(g.qubit_numbers[i] for i in range(g.num_qubits)),
+                    g.theta, g.phi, g.lambda_))
+    return out
 
 
 def add_gate_to_circuit_sys(circ, time, gate, *args, **kw):

@@ -244,7 +244,7 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8, tol=5
     evolved to t = 100 with its own Dormand-Prince 5(4) step at atol = rtol
     = tol): solves/s of the persistent batched kernel in FP64 and with
     complex64 right-hand-side increments (steps whose error estimate lies
-    within 0.5 of the accept threshold re-evaluated in complex128), against
+    within 0.1 of the accept threshold re-evaluated in complex128), against
     the plain path (time_step_sys, -ts_rk_type 5dp, one system at a time)
     timed on a sample, and the population error of the complex64 mode
     against the FP64 ensemble (which the parity tests hold to the oracle at

@@ -357,7 +357,7 @@ int quac_ensemble_get_states(quac_ensemble ens, PetscScalar *rho);
  * instance hit the step limit or a non-finite error norm. */
 int quac_ensemble_run(quac_ensemble ens, double t0, double tmax, double dt0);
 /* complex64 mode: a step whose error estimate lies within `margin` of the
- * accept threshold (|err - 1| < margin, default 0.5) is estimated again
+ * accept threshold (|err - 1| < margin, default 0.1) is estimated again
  * with complex128 stages, so the accept / reject decisions follow the
  * complex128 ones; 0 turns the re-evaluation off. */
 int quac_ensemble_set_redo_margin(quac_ensemble ens, double margin);
@@ -446,6 +446,13 @@ int quac_set_lrho_precision(int precision);
  * and also in quac_lrho_apply_device / quac_lrho_apply_host when x is
  * Hermitian to 1e-13; 0 = always compute every element. */
 int quac_set_hermitian_mode(int mode);
+/* Preconditioner of the steady-state GMRES (the role PCASM / ILU(0) plays in
+ * solver.c:167-198): 1 (default) = the exact inverse of the no-jump
+ * Liouvillian L0 X = -i (H_eff X - X H_eff^H), H_eff = H - i/2 sum a C^dag C,
+ * applied on the right through the eigen-decomposition of H_eff (computed
+ * once per system on the GPU; four D x D complex GEMMs per iteration);
+ * 0 = none.  The guided solve with a deflation space runs unpreconditioned. */
+int quac_set_gmres_preconditioner(int mode);
 /* Restart length of the steady-state GMRES (default 100 as in solver.c;
  * -ksp_gmres_restart on the QuaC_initialize command line does the same).
  * Up to 1024: a long Krylov space resolves the slow Lindblad modes that

@@ -186,6 +186,51 @@ def rk4(h, y0, dt, nsteps):
     return y
 
 
+def bs3_events(h, y0, t0, tmax, dt0, events, atol=5e-7, rtol=5e-7, hmin=0.01, hmax=1.0, max_steps=10 ** 9):
+    """Bogacki-Shampine 3(2) with the basic controller of time_step_sys
+    (qsystem.c:895-1098) and circuit events: a step that would pass the next
+    event time ends on it, the events at that time are applied in order
+    (event callables y -> y), and the controller continues from that step
+    (_sys_QC_EventFunction / PostEventFunction, quantum_circuits.c:17-120).
+    `events` is a list of (time, callable) sorted by time."""
+    y = np.array(y0, dtype=np.complex128, copy=True)
+    n = y.size
+    t, hh = t0, dt0
+    tol = 1e-12 * max(1.0, abs(tmax))
+    ev = [(te, f) for te, f in events if te > t0 and te <= tmax * (1 + 1e-14) + 1e-14]
+    k, steps = 0, 0
+    while steps < max_steps and t < tmax - tol:
+        h_try, last, at_event = hh, False, False
+        if t + h_try >= tmax - tol:
+            h_try, last = tmax - t, True
+        if k < len(ev) and t + h_try >= ev[k][0] - tol:
+            h_try, at_event, last = ev[k][0] - t, True, abs(ev[k][0] - tmax) <= tol
+        k1 = spmv(h, y)
+        k2 = spmv(h, y + 0.5 * h_try * k1)
+        k3 = spmv(h, y + 0.75 * h_try * k2)
+        yn = y + h_try * (2.0 / 9.0 * k1 + 1.0 / 3.0 * k2 + 4.0 / 9.0 * k3)
+        k4 = spmv(h, yn)
+        e = h_try * ((2.0 / 9.0 - 7.0 / 24.0) * k1 + (1.0 / 3.0 - 0.25) * k2 + (4.0 / 9.0 - 1.0 / 3.0) * k3
+                     - 0.125 * k4)
+        q = np.abs(e) / (atol + rtol * np.maximum(np.abs(y), np.abs(yn)))
+        err = np.sqrt(np.sum(q * q) / n)
+        fac = min(10.0, max(0.1, 0.9 * err ** (-1.0 / 3.0) if err > 0 else 10.0))
+        h_next = min(hmax, max(hmin, h_try * fac))
+        if not (err <= 1.0 or h_try <= hmin * (1 + 1e-12)):
+            hh = h_next
+            continue
+        y = yn
+        steps += 1
+        t = tmax if last else t + h_try
+        hh = h_next
+        if at_event:
+            te = ev[k][0]
+            while k < len(ev) and abs(ev[k][0] - te) <= tol:
+                y = ev[k][1](y)
+                k += 1
+    return y, steps
+
+
 def rk4_time_dep(h0, terms, y0, t0, dt, nsteps, min_time_dep=1e-10):
     """Classical RK4 on Y = A X + sum_k a_k f_k(t) A_k X, the matrix-shell
     product of qsystem.c:1300-1330: `h0` is the CSR of the time-independent

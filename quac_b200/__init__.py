@@ -167,6 +167,7 @@ def lib():
         "quac_set_kernel_path": (None, [ctypes.c_int]),
         "quac_set_lrho_precision": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_hermitian_mode": (ctypes.c_int, [ctypes.c_int]),
+        "quac_set_gmres_preconditioner": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_restart": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_precision": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_deflation_refresh": (ctypes.c_int, [ctypes.c_int]),
@@ -798,6 +799,13 @@ def set_deflation_refresh(mode):
     """1 (default): steady_state_guided rebuilds its deflation space from the
     iterate at every restart; 0: keeps the proposed one."""
     lib().quac_set_deflation_refresh(int(mode))
+    _check()
+
+
+def set_gmres_preconditioner(mode):
+    """1 (default): steady-state GMRES preconditioned by the exact inverse of
+    the no-jump Liouvillian; 0: none."""
+    lib().quac_set_gmres_preconditioner(int(mode))
     _check()
 
 

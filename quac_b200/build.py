@@ -58,7 +58,7 @@ def build(force=False, verbose=False, extra=()):
     objs = [o for o, _ in results]
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", CCBIN, "-o", LIB] + objs + ["-lcuda"]
+        cmd = [NVCC] + ARCH + ["-shared", "-ccbin", CCBIN, "-o", LIB] + objs + ["-lcuda", "-lcublas", "-lcusolver"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -282,6 +282,7 @@ void destroy_system(qsystem *qsys) {
   q->impl->obsmon.release();
   clear_mat_terms_sys(q);
   mcwf_release_system(q);
+  precond_release_system(q);
   q->impl->ws.release();
   if (q->impl->host_vec) vec_free(q->impl->host_vec);
   if (q->impl->ws.dsum) cudaFree(q->impl->ws.dsum);
@@ -1431,6 +1432,12 @@ extern "C" int quac_set_gmres_precision(int precision) {
 extern "C" int quac_set_deflation_refresh(int mode) {
   if (mode != 0 && mode != 1) { fail(0, "ERROR! deflation refresh must be 0 (off) or 1 (every restart)\n"); return 1; }
   options().defl_refresh = mode;
+  return 0;
+}
+
+extern "C" int quac_set_gmres_preconditioner(int mode) {
+  if (mode != 0 && mode != 1) { fail(0, "ERROR! GMRES preconditioner must be 0 (none) or 1 (no-jump inverse)\n"); return 1; }
+  options().gmres_precond = mode;
   return 0;
 }
 

@@ -66,6 +66,7 @@ struct Options {
   int gmres_f32 = 0;                // see quac_set_gmres_precision
   int defl_refresh = 1;             // see quac_set_deflation_refresh
   int gmres_restart = 100;          // -ksp_gmres_restart (solver.c uses PETSc's default 100 via KSPGMRESSetRestart)
+  int gmres_precond = 1;            // see quac_set_gmres_preconditioner
   bool rk4_classic = false;         // rk_type "4classic": four-stage form instead of Horner
 };
 Options &options();
@@ -113,6 +114,8 @@ bool mcwf_spawned(qvec q);
 void mcwf_release(qvec q);
 void mcwf_release_system(qsystem qs);
 cplx mcwf_expectation(qvec q, const int *map, const double2 *val);
+// steady-state preconditioner cache (precond.cu)
+void precond_release_system(qsystem qs);
 // device tables of the observable monitor's observables (capi.cpp)
 void observable_monitor_tables(qsystem qs, int64_t D);
 // small_run.cu

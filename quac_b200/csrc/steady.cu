@@ -753,6 +753,11 @@ static GmresSlot &gmres_slot() {
 
 static Gmres &gmres_for(qsystem) { return gmres_slot().g; }
 
+struct SteadyPrecond;
+SteadyPrecond *precond_for(qsystem qs, cudaStream_t s);
+void precond_apply(SteadyPrecond &P, const double2 *x, double2 *y, cudaStream_t s);
+double2 *precond_scratch(SteadyPrecond &P);
+
 // A x with A = L + e0 vec(I)^T
 static void apply_A(const DeviceProgram &PP, const double2 *x, double2 *y, cudaStream_t s) {
   Epi e;
@@ -1193,10 +1198,13 @@ static bool step_graph(Gmres &G, const DeviceProgram &PP, Deflation *def, int m,
 // STALL_CYCLES restarts earlier, and the caller continues in complex128.
 constexpr int STALL_CYCLES = 20;
 
+// With pre (right preconditioning, no deflation): the Arnoldi process runs
+// on A M^-1 and each cycle ends with x += M^-1 V y, so the residual it
+// minimises is still the true residual b - A x.
 template <typename VT>
 static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double rtol, int m, int64_t maxit,
                          double *final_res, Deflation *def, bool refresh, cudaStream_t s,
-                         bool *stalled = nullptr) {
+                         bool *stalled = nullptr, SteadyPrecond *pre = nullptr) {
   const int64_t n = G.n;
   VT *V = G.basis<VT>();
   std::vector<std::complex<double>> H((size_t)(m + 1) * m), cs(m), sn(m), gvec(m + 1), y(m);
@@ -1235,7 +1243,7 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
     // only V_j, which step j-1 scaled on the device, so the host queues
     // the next steps before it reads column j back and applies the Givens
     // rotations.  Steps queued past convergence are discarded.
-    const bool graph = G.small() && step_graph<VT>(G, PP, def, m, s);
+    const bool graph = G.small() && !pre && step_graph<VT>(G, PP, def, m, s);
     if (graph) QCUDA(cudaMemsetAsync(G.jdev, 0, sizeof(int), s));
     auto launch_step = [&](int j) {
       if (graph) {  // the step index advances on the device
@@ -1245,13 +1253,19 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
         return;
       }
       const VT *vj = V + (size_t)j * n;
+      const double2 *src;
       if constexpr (std::is_same<VT, double2>::value) {
-        apply_A(PP, reinterpret_cast<const double2 *>(vj), G.w, s);
+        src = reinterpret_cast<const double2 *>(vj);
       } else {
         k_scale<<<grid_for(n), NT, 0, s>>>(vj, G.t, n, 1.0);
         count_launch();
-        apply_A(PP, G.t, G.w, s);
+        src = G.t;
       }
+      if (pre) {  // w = A M^-1 v_j
+        precond_apply(*pre, src, precond_scratch(*pre), s);
+        src = precond_scratch(*pre);
+      }
+      apply_A(PP, src, G.w, s);
       if (def) apply_P(PP, *def, G.w, n, s);  // Arnoldi on P A
       // CGS2 on the device; the Hessenberg column (projections of both
       // passes summed, then ||w||) goes to ring slot j % GMRES_RING
@@ -1325,6 +1339,13 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
         apply_Q(*def, def->t2, def->t1, s);
         k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, def->t1, n, -1.0);
         count_launch();
+      } else if (pre) {  // x += M^-1 V y
+        QCUDA(cudaMemsetAsync(G.w, 0, n * sizeof(double2), s));
+        k_multiaxpy<<<grid_for(n), NT, 0, s>>>(V, G.h, n, j, G.w, 1.0);
+        count_launch();
+        precond_apply(*pre, G.w, precond_scratch(*pre), s);
+        k_axpy_inplace<<<grid_for(n), NT, 0, s>>>(x, precond_scratch(*pre), n, 1.0);
+        count_launch();
       } else {
         k_multiaxpy<<<grid_for(n), NT, 0, s>>>(V, G.h, n, j, x, 1.0);
         count_launch();
@@ -1356,11 +1377,18 @@ int64_t gmres_solve(qsystem qs, double2 *x, double rtol, int m, int64_t maxit, b
     const double2 one = make_double2(1.0, 0.0);
     QCUDA(cudaMemcpyAsync(x, &one, sizeof(double2), cudaMemcpyHostToDevice, s));
   }
-  if (!f32) return gmres_run<double2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s);
+  // the no-jump preconditioner (quac_set_gmres_preconditioner) in runs
+  // without a deflation space
+  SteadyPrecond *pre = nullptr;
+  if (options().gmres_precond && !def) {
+    pre = precond_for(qs, s);
+    if (!pre) return -1;
+  }
+  if (!f32) return gmres_run<double2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s, nullptr, pre);
   bool stalled = false;
-  int64_t its = gmres_run<float2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s, &stalled);
+  int64_t its = gmres_run<float2>(PP, G, x, rtol, m, maxit, final_res, def, refresh, s, &stalled, pre);
   if (!stalled || its < 0) return its;
-  const int64_t more = gmres_run<double2>(PP, G, x, rtol, m, maxit - its, final_res, def, refresh, s);
+  const int64_t more = gmres_run<double2>(PP, G, x, rtol, m, maxit - its, final_res, def, refresh, s, nullptr, pre);
   return more < 0 ? -1 : its + more;
 }
 

@@ -4,22 +4,20 @@ Pipeline (driven Tavis-Cummings sweep: Omega ~ U[0, 0.5], Delta ~ U[-1, 1],
 kappa ~ U[0.01, 0.2], gamma ~ U[1e-3, 1e-2], g = 0.1):
 
 1. training states come from the solver itself: points are visited along a
-   greedy nearest-neighbour chain; the first is solved cold (GMRES(100)
-   from e0), every later one starts from the rank-16 factors of the nearest
-   point solved so far and is deflated by their leading directions;
+   greedy nearest-neighbour chain; the first is solved from e0, every later
+   one starts from the rank-16 factors of the nearest point solved so far;
 2. the network (quac_wsnet_*) learns parameters -> rank-r factors F with
    F F^H ~ rho_ss;
-3. a new point is solved from the proposal: initial state F F^H / tr and
-   deflation space { u_i u_j^H } from the kd leading left singular vectors
-   of F (quac_steady_state_guided), plain GMRES as the fallback.
+3. a new point is solved from the proposal F F^H / tr.
 
-The guided solve projects the deflation space out of the Krylov process
-(Galerkin projection) and, by default, refreshes it at every restart from
-the iterate's leading eigenvectors, so a proposal that is only roughly
-right still converges toward the exact subspace; the proposal's value is
-in the first restarts.  The guided phase is capped and plain GMRES takes
-over from its iterate.  The residual ||(L + e0 vec(I)^T) rho - e0|| <= 1e-11
-decides every solve.
+With the steady-state preconditioner on (quac_set_gmres_preconditioner,
+the exact inverse of the no-jump Liouvillian) every solve is a
+preconditioned GMRES(100) started from the better of the proposal and e0.
+With it off, the proposal also supplies a deflation space { u_i u_j^H }
+from the kd leading left singular vectors of F (quac_steady_state_guided:
+Galerkin projection refreshed at every restart from the iterate), which
+is what makes unpreconditioned GMRES converge on these slow Liouvillians.
+The residual ||(L + e0 vec(I)^T) rho - e0|| <= 1e-11 decides every solve.
 """
 import argparse
 import sys
@@ -108,7 +106,7 @@ def solve_guided(q, theta, ne, nc, x0, U, maxit_guided=3000):
     return B, v, its, res, dt
 
 
-def generate(q, net, thetas, ne, nc, kd=8, rank=16, maxit_guided=3000, log=None):
+def generate(q, net, thetas, ne, nc, kd=8, rank=16, maxit_guided=3000, log=None, precond=False):
     """Solves every point and adds it to the network's samples; returns the
     iteration counts in visiting order."""
     D = 2 ** ne * nc
@@ -123,7 +121,7 @@ def generate(q, net, thetas, ne, nc, kd=8, rank=16, maxit_guided=3000, log=None)
             v.from_numpy(x)
         else:
             near = min(solved, key=lambda s: float(np.sum((s[0] - z[i]) ** 2)))
-            x0, U = proposal_from_factors(near[1], kd)
+            x0, U = proposal_from_factors(near[1], 0 if precond else kd)
             B, v, its, res, dt = solve_guided(q, thetas[i], ne, nc, x0, U, maxit_guided)
             x = v.to_numpy()
         net.add_sample(z[i], v)
@@ -152,7 +150,7 @@ def sweep_settings(**kw):
     steps and learning rate, guided-solver basis precision (fp32), deflation
     rank kd, restart length and refresh; kw overrides the defaults."""
     a = argparse.Namespace(ne=3, nc=4, train=48, held=12, sweep2d=False, steps=8000, lr=2e-3, fp32=1, kd=8,
-                           seed=5, restart=100, refresh=1)
+                           seed=5, restart=100, refresh=1, precond=0, cold_sample=None)
     for k, v in kw.items():
         setattr(a, k, v)
     return a
@@ -164,30 +162,37 @@ def measure_sweep(q, a):
     sweep_settings).  Training states are generated by the solver itself
     (generate), the network is trained on the GPU, then every held-out point
     is solved three ways, each to ||(L + e0 vec(I)^T) x - e0|| <= 1e-11:
-    cold, plain complex128 GMRES(100) from e0 (steady_state_sys); method,
-    the guided solver with the learned run's settings started from e0 with
-    the first kd unit vectors as U (the method without the network);
-    learned, the same solver started from the network's proposal.  Returns
-    solves/s of each, the ratios, iteration counts and the largest
-    population difference against the cold solve."""
+    cold, unpreconditioned complex128 GMRES(100) from e0 (on the first
+    a.cold_sample points when set); method, the learned run's solver
+    (a.precond: preconditioned GMRES(100); otherwise the guided solver with
+    the first kd unit vectors as deflation space) started from e0, i.e. the
+    method without the network; learned, the same solver started from the
+    network's proposal.  Returns solves/s of each, the ratios, iteration
+    counts and the largest population difference against the cold (or
+    method) solve."""
     WS = sys.modules[__name__]
     D = 2 ** a.ne * a.nc
+    kd = 0 if a.precond else a.kd
     fixed = {2: 0.1, 3: 5e-3} if a.sweep2d else None
     thetas = WS.sweep_params(a.train + a.held, seed=a.seed, fixed=fixed)
     train, held = thetas[:a.train], thetas[a.train:]
+    ncold = len(held) if a.cold_sample is None else min(len(held), a.cold_sample)
     net = q.WarmStartNet(D, rank=16, hidden=256, batch=min(128, a.train), max_samples=a.train, seed=2)
+
     def learned_settings():
-        q.set_gmres_precision(a.fp32)
-        q.set_gmres_restart(a.restart)
+        q.set_gmres_preconditioner(a.precond)
+        q.set_gmres_precision(0 if a.precond else a.fp32)
+        q.set_gmres_restart(100 if a.precond else a.restart)
         q.set_deflation_refresh(a.refresh)
 
     def plain_settings():
+        q.set_gmres_preconditioner(0)
         q.set_gmres_precision(0)
         q.set_gmres_restart(100)
 
     learned_settings()
     t = time.perf_counter()
-    gen_its = WS.generate(q, net, train, a.ne, a.nc, kd=a.kd)
+    gen_its = WS.generate(q, net, train, a.ne, a.nc, kd=kd, precond=bool(a.precond))
     t_gen = time.perf_counter() - t
     t = time.perf_counter()
     loss = net.train(a.steps, lr=a.lr, seed=3)
@@ -195,57 +200,66 @@ def measure_sweep(q, a):
 
     # untimed warm-up of every arm on a training point: the first solve of a
     # solver setting in a process loads its kernels and sizes its buffers
-    plain_settings()
-    WS.solve_cold(q, train[0], a.ne, a.nc)
+    if ncold:
+        plain_settings()
+        WS.solve_cold(q, train[0], a.ne, a.nc)
     learned_settings()
     e0 = np.zeros(D * D, complex)
     e0[0] = 1.0
-    for x0, U in ((e0, np.eye(D, a.kd, dtype=complex)),
-                  WS.proposal_from_factors(net.predict(WS.normalize(train[0])[None, :])[0], a.kd)):
+    for x0, U in ((e0, np.eye(D, kd, dtype=complex)),
+                  WS.proposal_from_factors(net.predict(WS.normalize(train[0])[None, :])[0], kd)):
         B, v, _, _, _ = WS.solve_guided(q, train[0], a.ne, a.nc, x0, U)
         v.destroy()
         B.qs.destroy()
 
     rows = []
-    for th in held:
-        plain_settings()
-        xc, its_c, dt_c = WS.solve_cold(q, th, a.ne, a.nc)
+    for k, th in enumerate(held):
+        xc, its_c, dt_c = None, -1, float("nan")
+        if k < ncold:
+            plain_settings()
+            xc, its_c, dt_c = WS.solve_cold(q, th, a.ne, a.nc)
         learned_settings()
-        B, v, its_m, _, dt_m = WS.solve_guided(q, th, a.ne, a.nc, e0, np.eye(D, a.kd, dtype=complex))
+        B, v, its_m, _, dt_m = WS.solve_guided(q, th, a.ne, a.nc, e0, np.eye(D, kd, dtype=complex))
         xm = v.to_numpy()
         v.destroy()
         B.qs.destroy()
         t = time.perf_counter()
-        x0, U = WS.proposal_from_factors(net.predict(WS.normalize(th)[None, :])[0], a.kd)
+        x0, U = WS.proposal_from_factors(net.predict(WS.normalize(th)[None, :])[0], kd)
         dt_p = time.perf_counter() - t
         B, v, its_l, res, dt_s = WS.solve_guided(q, th, a.ne, a.nc, x0, U)
         xl = v.to_numpy()
         v.destroy()
         B.qs.destroy()
         dt_l = dt_p + dt_s  # network inference + proposal + solve
-        pc = xc.reshape(D, D, order="F").diagonal().real
+        pc = (xc if xc is not None else xm).reshape(D, D, order="F").diagonal().real
         perr = max(np.abs(x.reshape(D, D, order="F").diagonal().real - pc).max() for x in (xm, xl))
         rows.append((its_c, dt_c, its_m, dt_m, its_l, dt_l, perr, res))
     plain_settings()
+    q.set_gmres_preconditioner(1)
     q.set_deflation_refresh(1)
     r = np.array(rows)
     n = len(held)
+    rc = r[:ncold]
     out = {
         "workload": f"tavis_cummings_steady_ne{a.ne}_nc{a.nc}_D{D}",
         "sweep": "2d (omega, delta)" if a.sweep2d else "4d (omega, delta, kappa, gamma)",
-        "train_states": a.train, "held_out": n, "kd": a.kd,
-        "solver": ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + f" GMRES({a.restart})"
-                  + (", deflation refreshed every restart" if a.refresh else ""),
+        "train_states": a.train, "held_out": n, "kd": kd,
+        "solver": ("no-jump-preconditioned fp64 GMRES(100)" if a.precond else
+                   ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + f" GMRES({a.restart})"
+                   + (", deflation refreshed every restart" if a.refresh else "")),
         "generation": {"seconds": t_gen, "mean_iterations": float(np.mean(gen_its))},
         "training": {"steps": a.steps, "seconds": t_train, "loss": loss},
-        "cold": {"solves_per_s": n / r[:, 1].sum(), "iterations": r[:, 0].astype(int).tolist()},
         "method": {"solves_per_s": n / r[:, 3].sum(), "iterations": r[:, 2].astype(int).tolist()},
         "learned": {"solves_per_s": n / r[:, 5].sum(), "iterations": r[:, 4].astype(int).tolist()},
-        "learned_vs_cold": r[:, 1].sum() / r[:, 5].sum(),
         "learned_vs_method": r[:, 3].sum() / r[:, 5].sum(),
-        "method_vs_cold": r[:, 1].sum() / r[:, 3].sum(),
         "pop_err_max": float(r[:, 6].max()),
         "residual_max": float(r[:, 7].max()),
     }
+    if ncold:
+        out["cold"] = {"solves_per_s": ncold / rc[:, 1].sum(), "iterations": rc[:, 0].astype(int).tolist(),
+                       "points": ncold}
+        # per-solve time ratios on the points every arm solved
+        out["learned_vs_cold"] = rc[:, 1].sum() / rc[:, 5].sum()
+        out["method_vs_cold"] = rc[:, 1].sum() / rc[:, 3].sum()
     net.destroy()
     return out

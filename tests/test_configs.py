@@ -306,3 +306,41 @@ def test_set_qvec_from_init_excited_op(quac):
     assert q.get_dm_element_qvec(rho, i, i) == 1.0
     rho.destroy()
     qs.destroy()
+
+
+def test_circuit_events_inside_time_step_match_oracle(quac, oracle):
+    """Gates scheduled at times inside one time_step_sys run (in-place
+    engine, quantum_circuits.c:17-120): the integration stops on every
+    event time, applies the gates and continues the same controller,
+    against the oracle's restatement (oracle.bs3_events) step for step."""
+    q = quac
+    S = H.ProductSystem(q)
+    O = oracle.OSys()
+    for T in (S, O):
+        qs_ = [T.op(2) for _ in range(3)]
+        T.ham(0.4, qs_[0].sig_x)
+        T.ham(0.25, qs_[1].sig_z, qs_[2].sig_z)
+        T.lin(0.05, qs_[0].a)
+        T.lin(0.02, qs_[2].n)
+    q.construct_matrix(S.qs)
+    rho = q.create_qvec_sys(S.qs)
+    q.add_to_qvec(rho, 1.0, 0, 0)
+    q.assemble_qvec(rho)
+    circ = q.create_circuit(5)
+    gates = [(0.3, "HADAMARD", (0,), {}), (0.3, "CNOT", (0, 2), {}), (0.85, "RY", (1,), dict(theta=0.7)),
+             (1.4, "U3", (2,), dict(theta=0.3, phi=1.1, lam=-0.4)), (1.4, "SIGMAX", (1,), {})]
+    for t, g, qb, kw in gates:
+        q.add_gate_to_circuit_sys(circ, t, g, *qb, **kw)
+    q.apply_circuit_to_sys(S.qs, circ, 0.0)
+    q.time_step_sys(S.qs, rho, 0.0, 2.0, 0.05, 10 ** 6)
+    dims = [2] * 6
+    evs = [(t, (lambda g, qb, kw: (lambda y: oracle.gate_inplace(dims, y, g, list(qb), **kw)))(g, qb, kw))
+           for t, g, qb, kw in gates]
+    h = O.csr_handle()
+    x0 = np.zeros(64, dtype=complex)
+    x0[0] = 1.0
+    yo, _ = oracle.bs3_events(h, x0, 0.0, 2.0, 0.05, evs)
+    oracle.free_csr(h)
+    assert _rel(rho.to_numpy(), yo) < 1e-10
+    rho.destroy()
+    S.qs.destroy()

@@ -120,12 +120,15 @@ def test_ensemble_fp32_rhs_population_error(quac, reference):
 @pytest.mark.parametrize("tol", [1e-10])
 def test_ensemble_fp32_rhs_within_1e8_of_oracle_at_tight_tolerance(quac, oracle, tol):
     """complex64 right-hand-side increments with the steps near the accept
-    threshold re-evaluated in complex128, at a tolerance where the
-    integration error itself is below the bar: every instance's populations
-    within 1e-8 of the oracle's complex128 DP5 at the same tolerance."""
+    threshold re-evaluated in complex128 (margin 0.5 here: every step
+    whose estimate is within a factor of two of the threshold), at a
+    tolerance where the integration error itself is below the bar: every
+    instance's populations within 1e-8 of the oracle's complex128 DP5 at the
+    same tolerance."""
     params = Sy.driven_jc_ensemble_params(64, seed=11, nc_lo=5, nc_hi=40)
     E, rho0 = _ensemble(quac, params)
     E.set_options(precision=1, atol=tol, rtol=tol)
+    E.set_redo_margin(0.5)
     E.set_states(rho0)
     E.run(0.0, T_END, DT0)
     y = E.get_states()

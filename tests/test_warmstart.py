@@ -266,6 +266,16 @@ def test_trained_network_proposals_and_measured_gain(quac):
     train, held = thetas[:48], thetas[48:]
     net = quac.WarmStartNet(D, rank=16, hidden=256, batch=64, max_samples=48, seed=2)
     untrained = quac.WarmStartNet(D, rank=16, hidden=256, batch=64, max_samples=1, seed=2)
+    quac.set_gmres_preconditioner(0)  # the deflation flow of unpreconditioned GMRES
+    try:
+        _run_deflation_flow(quac, WS, net, untrained, train, held, ne, nc, D)
+    finally:
+        quac.set_gmres_preconditioner(1)
+        net.destroy()
+        untrained.destroy()
+
+
+def _run_deflation_flow(quac, WS, net, untrained, train, held, ne, nc, D):
     WS.generate(quac, net, train, ne, nc, kd=8)
     loss = net.train(8000, lr=2e-3, seed=3)
     cold_its, learned_its, err_tr, err_un = [], [], [], []
@@ -285,5 +295,39 @@ def test_trained_network_proposals_and_measured_gain(quac):
           f"iterations cold {cold_its} learned {learned_its}")
     assert loss < 1e-2
     assert 3 * np.mean(err_tr) < np.mean(err_un)
+
+
+def test_learned_start_gain_over_method_with_preconditioner(quac):
+    """The preconditioned flow (the default): 48 solver-generated training
+    states of the (Omega, Delta) sweep, then every held-out point solved
+    from e0 (the method without the network) and from the trained network's
+    proposal, both by preconditioned GMRES(100) to the 1e-11 residual bar.
+    The network must save iterations: fewer in total over the held-out
+    points, and on every point no more than from e0."""
+    from quac_b200 import warmstart as WS
+    ne, nc = 3, 4
+    D = 2 ** ne * nc
+    thetas = WS.sweep_params(54, seed=5, fixed={2: 0.1, 3: 5e-3})
+    train, held = thetas[:48], thetas[48:]
+    net = quac.WarmStartNet(D, rank=16, hidden=256, batch=64, max_samples=48, seed=2)
+    WS.generate(quac, net, train, ne, nc, kd=0, precond=True)
+    net.train(8000, lr=2e-3, seed=3)
+    e0 = np.zeros(D * D, complex)
+    e0[0] = 1.0
+    its_m, its_l = [], []
+    for th in held:
+        B, v, im, rm, _ = WS.solve_guided(quac, th, ne, nc, e0, np.eye(D, 0, dtype=complex))
+        xm = v.to_numpy()
+        v.destroy()
+        B.qs.destroy()
+        xl, il, rl, _ = WS.solve_learned(quac, net, th, ne, nc, kd=0)
+        assert rm <= 1e-11 and rl <= 1e-11
+        pm = xm.reshape(D, D, order="F").diagonal().real
+        pl = xl.reshape(D, D, order="F").diagonal().real
+        assert np.abs(pl - pm).max() < 1e-8
+        its_m.append(im)
+        its_l.append(il)
+    print(f"preconditioned GMRES iterations: from e0 {its_m}, from the network's proposal {its_l}")
+    assert sum(its_l) < sum(its_m)
+    assert all(l <= m for l, m in zip(its_l, its_m))
     net.destroy()
-    untrained.destroy()

@@ -442,18 +442,21 @@ def circuit_summary(q, nq=10, layers=40):
 
 
 def steady_summary(q):
-    """Learned warm start for steady states, at the scale that fits the
-    bench: driven Tavis-Cummings with 3 emitters and 4 cavity levels
-    (D = 32), a 2-D sweep of (Omega, Delta), 48 solver-generated training
-    states, 12 held-out points.  Solves/s of plain complex128 GMRES(100)
-    from e0 against the learned start (FP32-inner / FP64-refined GMRES(300),
-    deflation refreshed every restart), and the same solver without the
-    network."""
-    from quac_b200 import warmstart
-    out = warmstart.measure_sweep(q, warmstart.sweep_settings(sweep2d=True, restart=300))
-    return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "solver", "cold", "method",
-                                "learned", "learned_vs_cold", "learned_vs_method", "method_vs_cold",
-                                "pop_err_max", "residual_max")}
+    """Steady states of driven Tavis-Cummings at the configuration's size:
+    6 emitters and 8 cavity levels (D = 512, Liouville dimension 262,144),
+    a 4-D sweep of (Omega, Delta, kappa, gamma); 100 solver-generated
+    training states and 20 held-out points (the configuration's 2,000 / 500
+    would take about 10 minutes of generation alone).  Solves/s of plain
+    complex128 GMRES(100) from e0 (one point: about 35 k iterations), of the
+    same GMRES preconditioned by the exact inverse of the no-jump
+    Liouvillian (the method, from e0) and of the learned start with the
+    preconditioned complex64-inner / complex128-refined solver."""
+    from quac_b200 import warmstart as WS
+    out = WS.measure_sweep(q, WS.sweep_settings(ne=6, nc=8, train=100, held=20, precond=1, cold_sample=1,
+                                                steps=4000, fp32=1))
+    return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "solver", "generation", "training",
+                                "cold", "method", "learned", "learned_vs_cold", "learned_vs_method",
+                                "method_vs_cold", "decompositions", "pop_err_max", "residual_max")}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -578,6 +581,7 @@ def run_profile(args):
       --profile ensemble --instances N --t-end T [--fp32]          one persistent ensemble launch
       --profile gemm     --m M --n N --k K --reps R                 TF32 tensor-core GEMM
       --profile steady   --ne E --nc C --train T --held H --kd K --restart M --fp32-basis B --sweep2d
+                         --precond P --cold-sample S --train-steps N   one steady-state sweep
                                                                      learned warm-start sweep
     """
     import ctypes
@@ -652,7 +656,8 @@ def run_profile(args):
     elif args.profile == "steady":
         from quac_b200 import warmstart
         a = warmstart.sweep_settings(ne=args.ne, nc=args.nc, train=args.train, held=args.held, kd=args.kd,
-                                     restart=args.restart, fp32=args.fp32_basis, sweep2d=args.sweep2d)
+                                     restart=args.restart, fp32=args.fp32_basis, sweep2d=args.sweep2d,
+                                     precond=args.precond, cold_sample=args.cold_sample, steps=args.train_steps)
         print(json.dumps(warmstart.measure_sweep(q, a)))
 
 
@@ -685,6 +690,9 @@ def main():
     ap.add_argument("--restart", type=int, default=300)
     ap.add_argument("--fp32-basis", type=int, default=1)
     ap.add_argument("--sweep2d", action="store_true")
+    ap.add_argument("--precond", type=int, default=1)
+    ap.add_argument("--cold-sample", type=int, default=None)
+    ap.add_argument("--train-steps", type=int, default=8000)
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

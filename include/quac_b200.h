@@ -302,9 +302,9 @@ int quac_lrho_apply_host(qsystem qsys, const PetscScalar *x_host, PetscScalar *y
  * stall other streams.  The multi-pass kernel's D^2 running sum lives in a
  * fixed 16 MiB device array, so qsys->dim may be at most 2^20 (10 qubits);
  * larger systems return an error.  Call quac_lrho_noalloc_setup(qsys) once,
- * with the system's device current, before the first apply and before any
- * stream capture: it may allocate (the system's term tables) and loads every
- * kernel the apply can launch, so that the apply itself allocates nothing.
+ * with the system's device current, before the first apply: it may allocate
+ * (the system's term tables) and loads every kernel the apply can launch, so
+ * that the apply itself allocates nothing.
  * The apply computes in the precision quac_set_lrho_precision selects, like
  * quac_lrho_apply_device, and returns once y is complete.  All systems on a
  * device share the one array: calls that overlap in time race and must be
@@ -453,6 +453,12 @@ int quac_set_hermitian_mode(int mode);
  * once per system on the GPU; four D x D complex GEMMs per iteration);
  * 0 = none.  The guided solve with a deflation space runs unpreconditioned. */
 int quac_set_gmres_preconditioner(int mode);
+/* No reference counterpart (PCSetUp builds PETSc's preconditioner the same
+ * way ahead of KSPSolve).  Builds qsys's steady-state preconditioner now;
+ * 0 on success. */
+int quac_steady_precond_setup(qsystem qsys);
+/* Decompositions computed in this process and their total host time (s). */
+void quac_steady_precond_stats(int64_t *builds, double *seconds);
 /* Restart length of the steady-state GMRES (default 100 as in solver.c;
  * -ksp_gmres_restart on the QuaC_initialize command line does the same).
  * Up to 1024: a long Krylov space resolves the slow Lindblad modes that

@@ -168,6 +168,8 @@ def lib():
         "quac_set_lrho_precision": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_hermitian_mode": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_preconditioner": (ctypes.c_int, [ctypes.c_int]),
+        "quac_steady_precond_setup": (ctypes.c_int, [P(_QsysStruct)]),
+        "quac_steady_precond_stats": (None, [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
         "quac_set_gmres_restart": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_precision": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_deflation_refresh": (ctypes.c_int, [ctypes.c_int]),
@@ -685,10 +687,9 @@ def add_gate_to_circuit_sys(circ, time, gate, *args, **kw):
     nq = _NQ[name]
     qubits, params = args[:nq], args[nq:]
     p = dict(theta=0.0, phi=0.0, lam=0.0)
-    if name in ("RX", "RY", "RZ"):
-        p["theta"] = params[0]
-    elif name in ("U1", "U2", "U3"):
-        p["theta"], p["phi"], p["lam"] = params
+    if len(params) > 3:
+        raise TypeError(f"{name}: at most three angles (theta, phi, lam), got {len(params)}")
+    p.update(zip(("theta", "phi", "lam"), params))
     p.update(kw)
     return circ.add_gate(time, g, *qubits, **p)
 
@@ -807,6 +808,20 @@ def set_gmres_preconditioner(mode):
     the no-jump Liouvillian; 0: none."""
     lib().quac_set_gmres_preconditioner(int(mode))
     _check()
+
+
+def steady_precond_setup(qs):
+    """Builds qs's steady-state preconditioner now (eigen-decomposition of
+    H_eff on the GPU)."""
+    lib().quac_steady_precond_setup(qs._ptr)
+    _check()
+
+
+def steady_precond_stats():
+    """(decompositions computed in this process, their total seconds)."""
+    n, sec = ctypes.c_int64(), ctypes.c_double()
+    lib().quac_steady_precond_stats(ctypes.byref(n), ctypes.byref(sec))
+    return n.value, sec.value
 
 
 def set_hermitian_mode(mode):

@@ -53,9 +53,6 @@ template <>
 __device__ __forceinline__ double2 to_v2<double2>(double2 v) { return v; }
 template <>
 __device__ __forceinline__ float2 to_v2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
-__device__ __forceinline__ double2 cmul2(double2 a, double2 b) {
-  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
 __device__ __forceinline__ double cabs2d(double2 a) { return sqrt(a.x * a.x + a.y * a.y); }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -181,14 +178,22 @@ __device__ __forceinline__ double2 stage_value(const Epi &E, int u, size_t idx, 
   return make_double2(fma(E.coef[u], Kv.x, b.x), fma(E.coef[u], Kv.y, b.y));
 }
 
-constexpr int QT = 512;          // threads of the pass kernel
-constexpr int QNW = QT / 32;     // warps
-constexpr int QMC = 64 / QNW;    // tile columns per thread
+#ifndef QUAC_QPASS_THREADS
+#define QUAC_QPASS_THREADS 512
+#endif
+constexpr int QT = QUAC_QPASS_THREADS;  // threads of the pass kernel (512 or 1024)
+constexpr int QNW = QT / 32;            // warps
+constexpr int QMC = 64 / QNW;           // tile columns per thread
+static_assert(QMC == 2 || QMC == 4, "pass kernel runs 512 or 1024 threads");
+// thread column m holds tile column w + QNW m: bit 0 of m is column bit
+// QCB, so flips of column bits >= QCB are register moves
+constexpr int QCB = QMC == 4 ? 4 : 5;
+__host__ __device__ constexpr int qcol_flip(int b) { return b >= QCB ? 1 << (b - QCB) : 0; }
 
 // One pass over 64 x 64 tiles.  Thread (lane, w) owns tile rows lane,
-// lane + 32 and columns w, w + 16, w + 32, w + 48; its eight values sit in
-// registers, so flips of row bit 5 and of column bits 4 and 5 need no
-// shared-memory read.  CANON (real mode only) is a compile-time mask of the
+// lane + 32 and columns w + QNW m (512 threads: w, w + 16, w + 32, w + 48);
+// its values sit in registers, so flips of row bit 5 and of the column bits
+// >= QCB need no shared-memory read.  CANON (real mode only) is a compile-time mask of the
 // canonical single-bit kinds present: 1 = left X, 2 = right X, 4 = lowering
 // jump, 8 = raising jump; CANON < 0 means the kinds are decided at run
 // time.  With TMA the CTAs are persistent, claim work items from a queue
@@ -367,7 +372,7 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
           for (int i = 0; i < 2; i++)
 #pragma unroll
             for (int m = 0; m < QMC; m++) {
-              const V2 p = b == 5 ? xo[i][m ^ 2] : (b == 4 ? xo[i][m ^ 1] : tile[(cl[m] ^ f) * 64 + rl[i]]);
+              const V2 p = b >= QCB ? xo[i][m ^ qcol_flip(b)] : tile[(cl[m] ^ f) * 64 + rl[i]];
               acc[i][m].x = fma(-hr, p.y, acc[i][m].x);
               acc[i][m].y = fma(hr, p.x, acc[i][m].y);
             }
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
             for (int m = 0; m < QMC; m++) {
               const bool rb = rl[i] & f, cb = cl[m] & f;
               const S g = (rb != cb) ? (S)0 : (rb ? gu : gl);
-              const V2 p = b == 5 ? xo[i ^ 1][m ^ 2] : tile[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
+              const V2 p = b == 5 ? xo[i ^ 1][m ^ qcol_flip(5)] : tile[(cl[m] ^ f) * 64 + (rl[i] ^ f)];
               acc[i][m].x = fma(g, p.x, acc[i][m].x);
               acc[i][m].y = fma(g, p.y, acc[i][m].y);
             }

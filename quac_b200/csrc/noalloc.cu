@@ -11,8 +11,8 @@
 //   - at most kNoAllocMaxElems = 2^20 complex values per vector (16 MiB of
 //     scratch: a 10-qubit density matrix); larger systems are rejected;
 //   - quac_lrho_noalloc_setup must be called once per system, with the
-//     system's device current, before the first apply and before any stream
-//     capture: it compiles the term program if needed, looks up the scratch
+//     system's device current, before the first apply: it compiles the
+//     term program if needed, looks up the scratch
 //     address of the current device and loads every kernel the apply can
 //     launch (CUDA's lazy module loading would otherwise load, and allocate
 //     device memory for, a kernel at its first launch);

@@ -12,15 +12,18 @@
 // Every eigenvalue of a dissipative H_eff has Im(lam) < 0, so the divisor
 // never vanishes; modes without decay get a small shift.  One application
 // is four D x D complex GEMMs (cuBLAS) and an element-wise scaling.  The
-// decomposition is computed once per system on the GPU (cuSOLVER geev and
-// an LU inverse of V) and cached by program serial number.
+// decomposition is computed on the GPU (cuSOLVER geev and an LU inverse of
+// V) once per system and cached by program serial number; at D = 512 it
+// takes about 0.14 s, most of a preconditioned solve.
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -30,27 +33,48 @@ namespace quac {
 
 bool compile_host(qsystem qs, int mode, HostProg &hp);
 
+// V, V^-1 and the eigenvalues of one H_eff (device memory)
+struct Decomp {
+  int D = 0;
+  int device = 0;
+  double shift = 0.0;
+  double2 *V = nullptr, *Vi = nullptr, *lam = nullptr;
+  ~Decomp() {
+    for (double2 *p : {V, Vi, lam})
+      if (p) cudaFree(p);
+  }
+};
+
+// per-device library handles and the scratch of precond_apply
+struct DeviceCtx {
+  cusolverDnHandle_t sol = nullptr;
+  cusolverDnParams_t par = nullptr;
+  cublasHandle_t blas = nullptr;
+  double2 *T = nullptr, *Z = nullptr;
+  size_t cap = 0;  // elements of T and Z
+};
+
 struct SteadyPrecond {
   uint64_t serial = 0;
-  int D = 0;
-  double2 *V = nullptr, *Vi = nullptr, *den = nullptr, *T = nullptr, *Z = nullptr;
-  cublasHandle_t blas = nullptr;
-  void release() {
-    for (double2 *p : {V, Vi, den, T, Z})
-      if (p) cudaFree(p);
-    V = Vi = den = T = Z = nullptr;
-    serial = 0;
-  }
+  std::shared_ptr<Decomp> dec;
+  DeviceCtx *ctx = nullptr;
 };
 
 namespace {
 
 constexpr int PT = 256;
 
-__global__ void k_hadamard(double2 *__restrict__ y, const double2 *__restrict__ den, int64_t n) {
+// y[k D + j] /= -i (lam_j - conj(lam_k)) - shift
+__global__ void k_sylvester_scale(double2 *__restrict__ y, const double2 *__restrict__ lam, int D, double shift) {
+  const int64_t n = (int64_t)D * D;
   for (int64_t i = (int64_t)blockIdx.x * PT + threadIdx.x; i < n; i += (int64_t)gridDim.x * PT) {
-    const double2 a = y[i], b = den[i];
-    y[i] = make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    const int k = (int)(i / D), j = (int)(i - (int64_t)k * D);
+    const double2 a = lam[j], b = lam[k];
+    // -i (a - conj(b)) = (a.y + b.y) - i (a.x - b.x)
+    const double dr = a.y + b.y - shift, di = b.x - a.x;
+    const double inv = 1.0 / (dr * dr + di * di);
+    const double2 v = y[i];
+    y[i] = make_double2((v.x * dr + v.y * di) * inv, (v.y * dr - v.x * di) * inv);
   }
 }
 
@@ -68,18 +92,38 @@ bool solver_ok(cusolverStatus_t st, const char *what) {
 
 std::mutex g_mu;
 std::map<qsystem, SteadyPrecond> g_pre;
+std::map<int, DeviceCtx> g_ctx;
+int64_t g_builds = 0;
+double g_build_seconds = 0.0;
 
-}  // namespace
+DeviceCtx *device_ctx() {
+  int dev = 0;
+  QCUDA(cudaGetDevice(&dev));
+  DeviceCtx &C = g_ctx[dev];
+  if (!C.sol) {
+    if (!solver_ok(cusolverDnCreate(&C.sol), "cusolverDnCreate")) { C.sol = nullptr; return nullptr; }
+    if (!solver_ok(cusolverDnCreateParams(&C.par), "cusolverDnCreateParams")) return nullptr;
+  }
+  if (!C.blas && !blas_ok(cublasCreate(&C.blas), "cublasCreate")) { C.blas = nullptr; return nullptr; }
+  return &C;
+}
 
-// Decomposes H_eff of qs (cached); nullptr on failure.
-SteadyPrecond *precond_for(qsystem qs, cudaStream_t s) {
-  ensure_program(qs);
-  if (has_error() || !qs->impl->prog) return nullptr;
-  std::lock_guard<std::mutex> lk(g_mu);
-  SteadyPrecond &P = g_pre[qs];
-  const uint64_t serial = qs->impl->prog->serial;
-  if (P.serial == serial && P.V) return &P;
-  P.release();
+bool ensure_scratch(DeviceCtx &C, size_t n2) {
+  if (C.cap >= n2) return true;
+  if (C.T) cudaFree(C.T);
+  if (C.Z) cudaFree(C.Z);
+  C.T = C.Z = nullptr;
+  C.cap = 0;
+  QCUDA(cudaMalloc(&C.T, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&C.Z, n2 * sizeof(double2)));
+  if (has_error()) return false;
+  C.cap = n2;
+  return true;
+}
+
+// eigen-decomposition of H_eff of qs (caller holds g_mu); nullptr on failure
+std::shared_ptr<Decomp> decompose(qsystem qs, DeviceCtx &C, cudaStream_t s) {
+  const auto t0 = std::chrono::steady_clock::now();
   HostProg hp;
   if (!compile_host(qs, 2, hp)) return nullptr;  // -i H_eff in Schroedinger form
   const int D = hp.D;
@@ -93,116 +137,148 @@ SteadyPrecond *precond_for(qsystem qs, cudaStream_t s) {
       const int c = hp.Lmap[t][r];
       if (c >= 0) H[(size_t)c * D + r] += I * hp.Lval[t][r];
     }
-  double2 *A = nullptr, *W = nullptr;
+  auto P = std::make_shared<Decomp>();
+  P->D = D;
+  QCUDA(cudaGetDevice(&P->device));
+  double2 *A = nullptr;
   int64_t *ipiv = nullptr;
   int *info = nullptr;
   void *dwork = nullptr;
-  QCUDA(cudaMalloc(&P.V, n2 * sizeof(double2)));
-  QCUDA(cudaMalloc(&P.Vi, n2 * sizeof(double2)));
-  QCUDA(cudaMalloc(&P.den, n2 * sizeof(double2)));
-  QCUDA(cudaMalloc(&P.T, n2 * sizeof(double2)));
-  QCUDA(cudaMalloc(&P.Z, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&P->V, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&P->Vi, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&P->lam, D * sizeof(double2)));
   QCUDA(cudaMalloc(&A, n2 * sizeof(double2)));
-  QCUDA(cudaMalloc(&W, D * sizeof(double2)));
   QCUDA(cudaMalloc(&ipiv, D * sizeof(int64_t)));
   QCUDA(cudaMalloc(&info, sizeof(int)));
-  QCUDA(cudaMemcpyAsync(A, H.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
-  cusolverDnHandle_t sol = nullptr;
-  cusolverDnParams_t par = nullptr;
-  bool ok = solver_ok(cusolverDnCreate(&sol), "cusolverDnCreate") && solver_ok(cusolverDnSetStream(sol, s), "stream") &&
-            solver_ok(cusolverDnCreateParams(&par), "params");
+  bool ok = !has_error() && ensure_scratch(C, n2);
+  if (ok) QCUDA(cudaMemcpyAsync(A, H.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ok = ok && solver_ok(cusolverDnSetStream(C.sol, s), "cusolverDnSetStream");
   size_t dsz = 0, hsz = 0, dsz2 = 0, hsz2 = 0;
   if (ok)
-    ok = solver_ok(cusolverDnXgeev_bufferSize(sol, par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D,
-                                              CUDA_C_64F, A, D, CUDA_C_64F, W, CUDA_C_64F, nullptr, D, CUDA_C_64F,
-                                              P.V, D, CUDA_C_64F, &dsz, &hsz),
+    ok = solver_ok(cusolverDnXgeev_bufferSize(C.sol, C.par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D,
+                                              CUDA_C_64F, A, D, CUDA_C_64F, P->lam, CUDA_C_64F, nullptr, D,
+                                              CUDA_C_64F, P->V, D, CUDA_C_64F, &dsz, &hsz),
                    "geev buffer size") &&
-         solver_ok(cusolverDnXgetrf_bufferSize(sol, par, D, D, CUDA_C_64F, P.Vi, D, CUDA_C_64F, &dsz2, &hsz2),
+         solver_ok(cusolverDnXgetrf_bufferSize(C.sol, C.par, D, D, CUDA_C_64F, P->Vi, D, CUDA_C_64F, &dsz2, &hsz2),
                    "getrf buffer size");
   std::vector<char> hwork(std::max(hsz, hsz2) + 1);
   if (ok) QCUDA(cudaMalloc(&dwork, std::max(dsz, dsz2) + 16));
   int hinfo = 0;
   if (ok && !has_error())
-    ok = solver_ok(cusolverDnXgeev(sol, par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D, CUDA_C_64F, A,
-                                   D, CUDA_C_64F, W, CUDA_C_64F, nullptr, D, CUDA_C_64F, P.V, D, CUDA_C_64F, dwork,
-                                   dsz, hwork.data(), hsz, info),
+    ok = solver_ok(cusolverDnXgeev(C.sol, C.par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D, CUDA_C_64F,
+                                   A, D, CUDA_C_64F, P->lam, CUDA_C_64F, nullptr, D, CUDA_C_64F, P->V, D, CUDA_C_64F,
+                                   dwork, dsz, hwork.data(), hsz, info),
                    "geev");
   if (ok) {
     QCUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
     QCUDA(cudaStreamSynchronize(s));
     if (hinfo != 0) { fail(9, "ERROR! eigen-decomposition of H_eff failed (info %d)\n", hinfo); ok = false; }
   }
-  // V^-1: LU of V (in Vi), then solve with the identity on the right
-  std::vector<std::complex<double>> Id(n2, 0.0);
-  for (int k = 0; k < D; k++) Id[(size_t)k * D + k] = 1.0;
+  // V^-1: LU of V (in A), then solve with the identity on the right (in Vi)
   if (ok) {
-    QCUDA(cudaMemcpyAsync(P.Vi, P.V, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-    QCUDA(cudaMemcpyAsync(P.T, Id.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
-    ok = solver_ok(cusolverDnXgetrf(sol, par, D, D, CUDA_C_64F, P.Vi, D, ipiv, CUDA_C_64F, dwork, dsz2, hwork.data(),
-                                    hsz2, info),
+    std::vector<std::complex<double>> Id(n2, 0.0);
+    for (int k = 0; k < D; k++) Id[(size_t)k * D + k] = 1.0;
+    QCUDA(cudaMemcpyAsync(A, P->V, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    QCUDA(cudaMemcpyAsync(P->Vi, Id.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ok = solver_ok(cusolverDnXgetrf(C.sol, C.par, D, D, CUDA_C_64F, A, D, ipiv, CUDA_C_64F, dwork, dsz2,
+                                    hwork.data(), hsz2, info),
                    "getrf") &&
-         solver_ok(cusolverDnXgetrs(sol, par, CUBLAS_OP_N, D, D, CUDA_C_64F, P.Vi, D, ipiv, CUDA_C_64F, P.T, D, info),
+         solver_ok(cusolverDnXgetrs(C.sol, C.par, CUBLAS_OP_N, D, D, CUDA_C_64F, A, D, ipiv, CUDA_C_64F, P->Vi, D,
+                                    info),
                    "getrs");
+    if (ok) {
+      QCUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+      QCUDA(cudaStreamSynchronize(s));  // also keeps Id alive until the copy is done
+      if (hinfo != 0) { fail(9, "ERROR! eigenvector matrix of H_eff is singular (info %d)\n", hinfo); ok = false; }
+    }
   }
   if (ok) {
-    QCUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
-    QCUDA(cudaStreamSynchronize(s));
-    if (hinfo != 0) { fail(9, "ERROR! eigenvector matrix of H_eff is singular (info %d)\n", hinfo); ok = false; }
-    std::swap(P.Vi, P.T);  // Vi = V^-1
-  }
-  if (ok) {
-    std::vector<std::complex<double>> lam(D), den(n2);
-    QCUDA(cudaMemcpy(lam.data(), W, D * sizeof(double2), cudaMemcpyDeviceToHost));
+    std::vector<std::complex<double>> lam(D);
+    QCUDA(cudaMemcpy(lam.data(), P->lam, D * sizeof(double2), cudaMemcpyDeviceToHost));
     double scale = 0.0;
     for (auto &l : lam) scale = std::max(scale, std::abs(l));
-    const double shift = 1e-8 * std::max(scale, 1e-300);  // modes without decay
-    for (int k = 0; k < D; k++)
-      for (int j = 0; j < D; j++) den[(size_t)k * D + j] = 1.0 / (-I * (lam[j] - std::conj(lam[k])) - shift);
-    QCUDA(cudaMemcpy(P.den, den.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice));
+    P->shift = 1e-8 * std::max(scale, 1e-300);  // modes without decay
   }
-  for (void *p : {(void *)A, (void *)W, (void *)ipiv, (void *)info, dwork})
+  for (void *p : {(void *)A, (void *)ipiv, (void *)info, dwork})
     if (p) cudaFree(p);
-  if (par) cusolverDnDestroyParams(par);
-  if (sol) cusolverDnDestroy(sol);
-  if (ok && !P.blas) ok = blas_ok(cublasCreate(&P.blas), "cublasCreate");
-  if (!ok || has_error()) {
-    P.release();
-    return nullptr;
-  }
-  P.D = D;
+  if (!ok || has_error()) return nullptr;
+  g_builds++;
+  g_build_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return P;
+}
+
+// the entry of qs, its decomposition valid for the current program
+SteadyPrecond *entry_for(qsystem qs, cudaStream_t s) {
+  ensure_program(qs);
+  if (has_error() || !qs->impl->prog) return nullptr;
+  DeviceCtx *C = device_ctx();
+  if (!C) return nullptr;
+  SteadyPrecond &P = g_pre[qs];
+  P.ctx = C;
+  const uint64_t serial = qs->impl->prog->serial;
+  if (P.serial == serial && P.dec) return ensure_scratch(*C, (size_t)P.dec->D * P.dec->D) ? &P : nullptr;
+  P.dec.reset();
+  P.serial = 0;
+  auto d = decompose(qs, *C, s);
+  if (!d) return nullptr;
+  P.dec = d;
   P.serial = serial;
   return &P;
 }
 
+}  // namespace
+
+// The preconditioner of qs (decomposed on first use)
+SteadyPrecond *precond_for(qsystem qs, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return entry_for(qs, s);
+}
+
 // y = L0^-1 x (vec of D x D, column stacking); x and y distinct
 void precond_apply(SteadyPrecond &P, const double2 *x, double2 *y, cudaStream_t s) {
-  const int D = P.D;
+  const Decomp &M = *P.dec;
+  const int D = M.D;
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
   auto *cx = reinterpret_cast<const cuDoubleComplex *>(x);
   auto *cy = reinterpret_cast<cuDoubleComplex *>(y);
-  auto *cT = reinterpret_cast<cuDoubleComplex *>(P.T);
-  auto *cV = reinterpret_cast<const cuDoubleComplex *>(P.V);
-  auto *cVi = reinterpret_cast<const cuDoubleComplex *>(P.Vi);
-  blas_ok(cublasSetStream(P.blas, s), "cublasSetStream");
+  auto *cT = reinterpret_cast<cuDoubleComplex *>(P.ctx->T);
+  auto *cV = reinterpret_cast<const cuDoubleComplex *>(M.V);
+  auto *cVi = reinterpret_cast<const cuDoubleComplex *>(M.Vi);
+  cublasHandle_t h = P.ctx->blas;
+  blas_ok(cublasSetStream(h, s), "cublasSetStream");
   // T = V^-1 X ;  Y = T V^-H ;  Y ./= den ;  T = V Y ;  Y = T V^H
-  blas_ok(cublasZgemm(P.blas, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one, cVi, D, cx, D, &zero, cT, D), "zgemm");
-  blas_ok(cublasZgemm(P.blas, CUBLAS_OP_N, CUBLAS_OP_C, D, D, D, &one, cT, D, cVi, D, &zero, cy, D), "zgemm");
+  blas_ok(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one, cVi, D, cx, D, &zero, cT, D), "zgemm");
+  blas_ok(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, D, D, D, &one, cT, D, cVi, D, &zero, cy, D), "zgemm");
   const int64_t n2 = (int64_t)D * D;
-  k_hadamard<<<(int)std::min<int64_t>((n2 + PT - 1) / PT, 148 * 8), PT, 0, s>>>(y, P.den, n2);
+  k_sylvester_scale<<<(int)std::min<int64_t>((n2 + PT - 1) / PT, 148 * 8), PT, 0, s>>>(y, M.lam, D, M.shift);
   count_launch();
-  blas_ok(cublasZgemm(P.blas, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one, cV, D, cy, D, &zero, cT, D), "zgemm");
-  blas_ok(cublasZgemm(P.blas, CUBLAS_OP_N, CUBLAS_OP_C, D, D, D, &one, cT, D, cV, D, &zero, cy, D), "zgemm");
+  blas_ok(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one, cV, D, cy, D, &zero, cT, D), "zgemm");
+  blas_ok(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, D, D, D, &one, cT, D, cV, D, &zero, cy, D), "zgemm");
 }
 
-double2 *precond_scratch(SteadyPrecond &P) { return P.Z; }
+double2 *precond_scratch(SteadyPrecond &P) { return P.ctx->Z; }
 
 void precond_release_system(qsystem qs) {
   std::lock_guard<std::mutex> lk(g_mu);
-  auto it = g_pre.find(qs);
-  if (it == g_pre.end()) return;
-  it->second.release();
-  if (it->second.blas) cublasDestroy(it->second.blas);
-  g_pre.erase(it);
+  g_pre.erase(qs);
 }
 
 }  // namespace quac
+
+using namespace quac;
+
+// Builds the steady-state preconditioner of qs now (the first
+// preconditioned solve would otherwise do it), like PCSetUp.
+extern "C" int quac_steady_precond_setup(qsystem qs) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!qs->mat_allocated) construct_matrix(qs);
+  if (has_error()) return 1;
+  return entry_for(qs, stream_of(qs)) ? 0 : 1;
+}
+
+// Decompositions computed in this process and their total host wall time.
+extern "C" void quac_steady_precond_stats(int64_t *builds, double *seconds) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (builds) *builds = g_builds;
+  if (seconds) *seconds = g_build_seconds;
+}

@@ -12,12 +12,15 @@ kappa ~ U[0.01, 0.2], gamma ~ U[1e-3, 1e-2], g = 0.1):
 
 With the steady-state preconditioner on (quac_set_gmres_preconditioner,
 the exact inverse of the no-jump Liouvillian) every solve is a
-preconditioned GMRES(100) started from the better of the proposal and e0.
-With it off, the proposal also supplies a deflation space { u_i u_j^H }
-from the kd leading left singular vectors of F (quac_steady_state_guided:
-Galerkin projection refreshed at every restart from the iterate), which
-is what makes unpreconditioned GMRES converge on these slow Liouvillians.
-The residual ||(L + e0 vec(I)^T) rho - e0|| <= 1e-11 decides every solve.
+preconditioned GMRES(100) started from the better of the proposal and e0;
+the eigen-decomposition behind the preconditioner is most of such a solve
+at D = 512 and the proposal cannot shorten it.  With the preconditioner
+off, the proposal also supplies a deflation space
+{ u_i u_j^H } from the kd leading left singular vectors of F
+(quac_steady_state_guided: Galerkin projection refreshed at every restart
+from the iterate), which is what makes unpreconditioned GMRES converge on
+these slow Liouvillians.  The residual ||(L + e0 vec(I)^T) rho - e0|| <=
+1e-11 decides every solve.
 """
 import argparse
 import sys
@@ -97,6 +100,8 @@ def solve_cold(q, theta, ne, nc):
 
 
 def solve_guided(q, theta, ne, nc, x0, U, maxit_guided=3000):
+    """Steady state of one point from x0 (deflation space U, or none when U
+    has no columns)."""
     B = build_tc(q, theta, ne, nc)
     v = q.create_qvec_sys(B.qs)
     v.from_numpy(x0)
@@ -161,15 +166,23 @@ def measure_sweep(q, a):
     against cold GMRES on held-out parameter points (`a` from
     sweep_settings).  Training states are generated by the solver itself
     (generate), the network is trained on the GPU, then every held-out point
-    is solved three ways, each to ||(L + e0 vec(I)^T) x - e0|| <= 1e-11:
-    cold, unpreconditioned complex128 GMRES(100) from e0 (on the first
-    a.cold_sample points when set); method, the learned run's solver
-    (a.precond: preconditioned GMRES(100); otherwise the guided solver with
-    the first kd unit vectors as deflation space) started from e0, i.e. the
-    method without the network; learned, the same solver started from the
-    network's proposal.  Returns solves/s of each, the ratios, iteration
-    counts and the largest population difference against the cold (or
-    method) solve."""
+    is solved by each arm, each to ||(L + e0 vec(I)^T) x - e0|| <= 1e-11:
+
+    cold     unpreconditioned complex128 GMRES(100) from e0 (on the first
+             a.cold_sample points when set), the plain path;
+    method   the learned run's solver without the network: with a.precond,
+             complex128 GMRES(100) preconditioned by the point's own
+             eigen-decomposition; otherwise the guided solver with the first
+             kd unit vectors as deflation space; both from e0;
+    learned  the network's proposal as start (the better of it and e0 by
+             residual), with a.precond preconditioned GMRES(100) in the
+             a.fp32 basis precision, otherwise with the proposal's deflation
+             space; its time includes inference and the proposal.
+
+    Every arm builds its own system (and with a.precond its own
+    decomposition, inside the timed solve).  Returns solves/s and
+    iterations of each arm, the ratios, and the largest population
+    difference and residual."""
     WS = sys.modules[__name__]
     D = 2 ** a.ne * a.nc
     kd = 0 if a.precond else a.kd
@@ -181,15 +194,21 @@ def measure_sweep(q, a):
 
     def learned_settings():
         q.set_gmres_preconditioner(a.precond)
-        q.set_gmres_precision(0 if a.precond else a.fp32)
+        q.set_gmres_precision(a.fp32)
         q.set_gmres_restart(100 if a.precond else a.restart)
         q.set_deflation_refresh(a.refresh)
+
+    def method_settings():
+        learned_settings()
+        if a.precond:
+            q.set_gmres_precision(0)
 
     def plain_settings():
         q.set_gmres_preconditioner(0)
         q.set_gmres_precision(0)
         q.set_gmres_restart(100)
 
+    builds0 = q.steady_precond_stats()
     learned_settings()
     t = time.perf_counter()
     gen_its = WS.generate(q, net, train, a.ne, a.nc, kd=kd, precond=bool(a.precond))
@@ -198,42 +217,50 @@ def measure_sweep(q, a):
     loss = net.train(a.steps, lr=a.lr, seed=3)
     t_train = time.perf_counter() - t
 
+    e0 = np.zeros(D * D, complex)
+    e0[0] = 1.0
+    U0 = np.eye(D, kd, dtype=complex)
+
+    def arm_method(th):
+        method_settings()
+        return WS.solve_guided(q, th, a.ne, a.nc, e0, U0)
+
+    def arm_learned(th):
+        learned_settings()
+        t0 = time.perf_counter()
+        x0, U = WS.proposal_from_factors(net.predict(WS.normalize(th)[None, :])[0], kd)
+        dt_p = time.perf_counter() - t0
+        B, v, its, res, dt = WS.solve_guided(q, th, a.ne, a.nc, x0, U)
+        return B, v, its, res, dt + dt_p  # network inference + proposal + solve
+
+    def finish(r):
+        B, v, its, res, dt = r
+        x = v.to_numpy()
+        v.destroy()
+        B.qs.destroy()
+        return x, its, res, dt
+
     # untimed warm-up of every arm on a training point: the first solve of a
     # solver setting in a process loads its kernels and sizes its buffers
     if ncold:
         plain_settings()
         WS.solve_cold(q, train[0], a.ne, a.nc)
-    learned_settings()
-    e0 = np.zeros(D * D, complex)
-    e0[0] = 1.0
-    for x0, U in ((e0, np.eye(D, kd, dtype=complex)),
-                  WS.proposal_from_factors(net.predict(WS.normalize(train[0])[None, :])[0], kd)):
-        B, v, _, _, _ = WS.solve_guided(q, train[0], a.ne, a.nc, x0, U)
-        v.destroy()
-        B.qs.destroy()
+    finish(arm_method(train[0]))
+    finish(arm_learned(train[0]))
 
+    builds1 = q.steady_precond_stats()
     rows = []
     for k, th in enumerate(held):
         xc, its_c, dt_c = None, -1, float("nan")
         if k < ncold:
             plain_settings()
             xc, its_c, dt_c = WS.solve_cold(q, th, a.ne, a.nc)
-        learned_settings()
-        B, v, its_m, _, dt_m = WS.solve_guided(q, th, a.ne, a.nc, e0, np.eye(D, kd, dtype=complex))
-        xm = v.to_numpy()
-        v.destroy()
-        B.qs.destroy()
-        t = time.perf_counter()
-        x0, U = WS.proposal_from_factors(net.predict(WS.normalize(th)[None, :])[0], kd)
-        dt_p = time.perf_counter() - t
-        B, v, its_l, res, dt_s = WS.solve_guided(q, th, a.ne, a.nc, x0, U)
-        xl = v.to_numpy()
-        v.destroy()
-        B.qs.destroy()
-        dt_l = dt_p + dt_s  # network inference + proposal + solve
+        xm, its_m, res_m, dt_m = finish(arm_method(th))
+        xl, its_l, res_l, dt_l = finish(arm_learned(th))
         pc = (xc if xc is not None else xm).reshape(D, D, order="F").diagonal().real
         perr = max(np.abs(x.reshape(D, D, order="F").diagonal().real - pc).max() for x in (xm, xl))
-        rows.append((its_c, dt_c, its_m, dt_m, its_l, dt_l, perr, res))
+        rows.append((its_c, dt_c, its_m, dt_m, its_l, dt_l, perr, max(res_m, res_l)))
+    builds2 = q.steady_precond_stats()
     plain_settings()
     q.set_gmres_preconditioner(1)
     q.set_deflation_refresh(1)
@@ -244,7 +271,9 @@ def measure_sweep(q, a):
         "workload": f"tavis_cummings_steady_ne{a.ne}_nc{a.nc}_D{D}",
         "sweep": "2d (omega, delta)" if a.sweep2d else "4d (omega, delta, kappa, gamma)",
         "train_states": a.train, "held_out": n, "kd": kd,
-        "solver": ("no-jump-preconditioned fp64 GMRES(100)" if a.precond else
+        "solver": ("GMRES(100) preconditioned by the exact inverse of the no-jump Liouvillian, "
+                   + ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + " basis in the learned arm"
+                   if a.precond else
                    ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + f" GMRES({a.restart})"
                    + (", deflation refreshed every restart" if a.refresh else "")),
         "generation": {"seconds": t_gen, "mean_iterations": float(np.mean(gen_its))},
@@ -255,6 +284,10 @@ def measure_sweep(q, a):
         "pop_err_max": float(r[:, 6].max()),
         "residual_max": float(r[:, 7].max()),
     }
+    if a.precond:
+        nb = builds2[0] - builds0[0]
+        out["decompositions"] = {"held_out": builds2[0] - builds1[0], "total": nb,
+                                 "mean_seconds": (builds2[1] - builds0[1]) / max(1, nb)}
     if ncold:
         out["cold"] = {"solves_per_s": ncold / rc[:, 1].sum(), "iterations": rc[:, 0].astype(int).tolist(),
                        "points": ncold}

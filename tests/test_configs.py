@@ -327,7 +327,7 @@ def test_circuit_events_inside_time_step_match_oracle(quac, oracle):
     q.add_to_qvec(rho, 1.0, 0, 0)
     q.assemble_qvec(rho)
     circ = q.create_circuit(5)
-    gates = [(0.3, "HADAMARD", (0,), {}), (0.3, "CNOT", (0, 2), {}), (0.85, "RY", (1,), dict(theta=0.7)),
+    gates = [(0.3, "HADAMARD", (0,), {}), (0.3, "CNOT", (0, 2), {}), (0.85, "RZ", (1,), dict(theta=0.7)),
              (1.4, "U3", (2,), dict(theta=0.3, phi=1.1, lam=-0.4)), (1.4, "SIGMAX", (1,), {})]
     for t, g, qb, kw in gates:
         q.add_gate_to_circuit_sys(circ, t, g, *qb, **kw)
@@ -342,5 +342,12 @@ def test_circuit_events_inside_time_step_match_oracle(quac, oracle):
     yo, _ = oracle.bs3_events(h, x0, 0.0, 2.0, 0.05, evs)
     oracle.free_csr(h)
     assert _rel(rho.to_numpy(), yo) < 1e-10
+    # RY has no in-place form in the reference either
+    # (quantum_circuits.c:3007-3035): the run stops with its message
+    bad = q.create_circuit(1)
+    q.add_gate_to_circuit_sys(bad, 2.5, "RY", 1, theta=0.7)
+    q.apply_circuit_to_sys(S.qs, bad, 0.0)
+    with pytest.raises(q.QuacError, match="get_gate_func_wf"):
+        q.time_step_sys(S.qs, rho, 2.0, 3.0, 0.05, 10 ** 6)
     rho.destroy()
     S.qs.destroy()

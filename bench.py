@@ -450,11 +450,14 @@ def steady_summary(q):
     complex128 GMRES(100) from e0 (one point: about 35 k iterations), of the
     same GMRES preconditioned by the exact inverse of the no-jump
     Liouvillian (the method, from e0) and of the learned start with the
-    preconditioned complex64-inner / complex128-refined solver."""
+    preconditioned complex64-inner / complex128-refined solver; every solve
+    to ||b - A x|| <= 1e-12 (tighter than the configuration's 1e-10, so
+    that the arms agree on populations to 1e-8)."""
     from quac_b200 import warmstart as WS
     out = WS.measure_sweep(q, WS.sweep_settings(ne=6, nc=8, train=100, held=20, precond=1, cold_sample=1,
-                                                steps=4000, fp32=1))
-    return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "solver", "generation", "training",
+                                                steps=4000, fp32=1, rtol=1e-12))
+    return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "rtol", "solver", "generation",
+                                "training",
                                 "cold", "method", "learned", "learned_vs_cold", "learned_vs_method",
                                 "method_vs_cold", "decompositions", "pop_err_max", "residual_max")}
 

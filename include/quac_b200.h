@@ -453,6 +453,10 @@ int quac_set_hermitian_mode(int mode);
  * once per system on the GPU; four D x D complex GEMMs per iteration);
  * 0 = none.  The guided solve with a deflation space runs unpreconditioned. */
 int quac_set_gmres_preconditioner(int mode);
+/* Tolerance of the steady-state GMRES on the true residual ||b - A x||
+ * with ||b|| = 1 (default 1e-11 as solver.c:14, 179; -ksp_rtol on the
+ * QuaC_initialize command line does the same). */
+int quac_set_gmres_tolerance(double rtol);
 /* No reference counterpart (PCSetUp builds PETSc's preconditioner the same
  * way ahead of KSPSolve).  Builds qsys's steady-state preconditioner now;
  * 0 on success. */

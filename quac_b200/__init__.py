@@ -169,6 +169,7 @@ def lib():
         "quac_set_hermitian_mode": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_preconditioner": (ctypes.c_int, [ctypes.c_int]),
         "quac_steady_precond_setup": (ctypes.c_int, [P(_QsysStruct)]),
+        "quac_set_gmres_tolerance": (ctypes.c_int, [dbl]),
         "quac_steady_precond_stats": (None, [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
         "quac_set_gmres_restart": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_precision": (ctypes.c_int, [ctypes.c_int]),
@@ -807,6 +808,12 @@ def set_gmres_preconditioner(mode):
     """1 (default): steady-state GMRES preconditioned by the exact inverse of
     the no-jump Liouvillian; 0: none."""
     lib().quac_set_gmres_preconditioner(int(mode))
+    _check()
+
+
+def set_gmres_tolerance(rtol):
+    """Steady-state GMRES tolerance on ||b - A x|| (default 1e-11)."""
+    lib().quac_set_gmres_tolerance(float(rtol))
     _check()
 
 

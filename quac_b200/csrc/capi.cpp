@@ -204,6 +204,7 @@ void QuaC_initialize(int argc, char **args) {
     else if (!strcmp(a, "-ts_atol")) { o.atol = atof(v); o.atol_set = true; i++; }
     else if (!strcmp(a, "-ts_max_steps")) { o.max_steps = atoll(v); i++; }
     else if (!strcmp(a, "-ksp_gmres_restart")) { o.gmres_restart = atoi(v); i++; }
+    else if (!strcmp(a, "-ksp_rtol")) { o.gmres_rtol = atof(v); i++; }
   }
 }
 
@@ -1432,6 +1433,12 @@ extern "C" int quac_set_gmres_precision(int precision) {
 extern "C" int quac_set_deflation_refresh(int mode) {
   if (mode != 0 && mode != 1) { fail(0, "ERROR! deflation refresh must be 0 (off) or 1 (every restart)\n"); return 1; }
   options().defl_refresh = mode;
+  return 0;
+}
+
+extern "C" int quac_set_gmres_tolerance(double rtol) {
+  if (!(rtol > 0.0 && rtol < 1.0)) { fail(0, "ERROR! GMRES tolerance must lie in (0, 1)\n"); return 1; }
+  options().gmres_rtol = rtol;
   return 0;
 }
 

@@ -1404,7 +1404,7 @@ extern "C" PetscInt steady_state_sys(qsystem qs, qvec x) {
   vec_sync_to_device(x->data);
   std::lock_guard<std::mutex> lk(gmres_slot().mu);
   double res = 0;
-  const int64_t its = gmres_solve(qs, x->data->d, 1e-11, options().gmres_restart, 200000, false, &res);
+  const int64_t its = gmres_solve(qs, x->data->d, options().gmres_rtol, options().gmres_restart, 200000, false, &res);
   return has_error() ? -1 : its;
 }
 
@@ -1464,11 +1464,12 @@ extern "C" PetscInt quac_steady_state_guided(qsystem qs, qvec x, const PetscScal
   }
   double res = 0;
   const int m = options().gmres_restart;
-  int64_t its = gmres_solve(qs, x->data->d, 1e-11, m, maxit_guided, true, &res, use ? &F : nullptr,
+  const double rtol = options().gmres_rtol;
+  int64_t its = gmres_solve(qs, x->data->d, rtol, m, maxit_guided, true, &res, use ? &F : nullptr,
                             options().defl_refresh != 0);
   if (its < 0) return -1;
-  if (res > 1e-11) {
-    const int64_t more = gmres_solve(qs, x->data->d, 1e-11, m, 200000, true, &res);
+  if (res > rtol) {
+    const int64_t more = gmres_solve(qs, x->data->d, rtol, m, 200000, true, &res);
     if (more < 0) return -1;
     its += more;
   }

@@ -153,9 +153,10 @@ def sweep_settings(**kw):
     """Settings of measure_sweep: ne emitters, nc cavity levels, train / held
     parameter points, 2-D sweep (kappa and gamma fixed), network training
     steps and learning rate, guided-solver basis precision (fp32), deflation
-    rank kd, restart length and refresh; kw overrides the defaults."""
+    rank kd, restart length and refresh, preconditioner, cold sample size
+    and GMRES tolerance; kw overrides the defaults."""
     a = argparse.Namespace(ne=3, nc=4, train=48, held=12, sweep2d=False, steps=8000, lr=2e-3, fp32=1, kd=8,
-                           seed=5, restart=100, refresh=1, precond=0, cold_sample=None)
+                           seed=5, restart=100, refresh=1, precond=0, cold_sample=None, rtol=1e-11)
     for k, v in kw.items():
         setattr(a, k, v)
     return a
@@ -209,6 +210,7 @@ def measure_sweep(q, a):
         q.set_gmres_restart(100)
 
     builds0 = q.steady_precond_stats()
+    q.set_gmres_tolerance(a.rtol)
     learned_settings()
     t = time.perf_counter()
     gen_its = WS.generate(q, net, train, a.ne, a.nc, kd=kd, precond=bool(a.precond))
@@ -264,13 +266,14 @@ def measure_sweep(q, a):
     plain_settings()
     q.set_gmres_preconditioner(1)
     q.set_deflation_refresh(1)
+    q.set_gmres_tolerance(1e-11)
     r = np.array(rows)
     n = len(held)
     rc = r[:ncold]
     out = {
         "workload": f"tavis_cummings_steady_ne{a.ne}_nc{a.nc}_D{D}",
         "sweep": "2d (omega, delta)" if a.sweep2d else "4d (omega, delta, kappa, gamma)",
-        "train_states": a.train, "held_out": n, "kd": kd,
+        "train_states": a.train, "held_out": n, "kd": kd, "rtol": a.rtol,
         "solver": ("GMRES(100) preconditioned by the exact inverse of the no-jump Liouvillian, "
                    + ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + " basis in the learned arm"
                    if a.precond else

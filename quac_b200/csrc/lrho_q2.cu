@@ -99,11 +99,6 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
-// bulk prefetch of [p, p + bytes) into L2 (16-byte aligned, bytes a multiple of 16)
-__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
-}
-
 // triangular work index t = b (b + 1) / 2 + a  ->  (a, b), a <= b
 __device__ __forceinline__ void tri_index(long long t, unsigned &a, unsigned &b) {
   long long J = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
@@ -256,29 +251,12 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
     const long long t = TMA ? tids[it % nst] : t_static;
     if (t >= P.ntiles) break;
     double2 *cur = sm + (it % nst) * NEL;
-    if (TMA && w == 0) {
-      long long t2 = 0;
-      if (lane == 0) {
-        const int q2 = (it + nst - 1) % nst;
-        t2 = (long long)atomicAdd(P.claim, 1ull);
-        tids[q2] = t2;
-        if (t2 < P.ntiles) tma_tile(P, &tmap, sm + q2 * NEL, &bars[q2], t2);
-        if (bt) tma_tile(P, &bmap, sm + 2 * NEL, &bars[3], t);
-      }
-      if (P.last && lo == 0 && P.accin) {
-        // the next item's running sum and first stage base are read at its
-        // start: bring their 1-KB columns into L2 now
-        t2 = __shfl_sync(0xffffffffu, t2, 0);
-        if (t2 < P.ntiles) {
-          unsigned r2, c2;
-          tile_origin(P, t2, r2, c2);
-          for (int k = lane; k < TILE; k += 32) {
-            const size_t e0 = (size_t)(c2 | (unsigned)k) * D + r2;
-            prefetch_l2(reinterpret_cast<const V2 *>(P.accin) + e0, TILE * sizeof(V2));
-            if (bt) prefetch_l2(E.base[0] + e0, TILE * sizeof(double2));
-          }
-        }
-      }
+    if (TMA && threadIdx.x == 0) {
+      const int q2 = (it + nst - 1) % nst;
+      const long long t2 = (long long)atomicAdd(P.claim, 1ull);
+      tids[q2] = t2;
+      if (t2 < P.ntiles) tma_tile(P, &tmap, sm + q2 * NEL, &bars[q2], t2);
+      if (bt) tma_tile(P, &bmap, sm + 2 * NEL, &bars[3], t);
     }
     unsigned rfix, cfix;
     tile_origin(P, t, rfix, cfix);

@@ -244,7 +244,9 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8, tol=5
     evolved to t = 100 with its own Dormand-Prince 5(4) step at atol = rtol
     = tol): solves/s of the persistent batched kernel in FP64 and with
     complex64 right-hand-side increments (steps whose error estimate lies
-    within 0.1 of the accept threshold re-evaluated in complex128), against
+    within 0.1 of the accept threshold re-evaluated in complex128, and an
+    instance whose estimated accumulated complex64 error passes 1e-9
+    continued in complex128), against
     the plain path (time_step_sys, -ts_rk_type 5dp, one system at a time)
     timed on a sample, and the population error of the complex64 mode
     against the FP64 ensemble (which the parity tests hold to the oracle at
@@ -277,6 +279,9 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8, tol=5
         if mode == 1:
             red = E.redone_steps()
             out[name]["redone_step_fraction"] = float(red.sum() / max(1.0, (st[:, 1] + st[:, 2]).sum()))
+            f64 = E.f64_steps()
+            out[name]["complex128_step_fraction"] = float(f64.sum() / max(1.0, st[:, 1].sum()))
+            out[name]["instances_switched_to_complex128"] = int((f64 > 0).sum())
     pops = lambda x, i: E.state(x, i).diagonal().real
     err = np.array([np.abs(pops(states[0], i) - pops(states[1], i)).max() for i in range(n_inst)])
     out["fp32_rhs"]["pop_err_vs_fp64"] = {"median": float(np.median(err)), "p99": float(np.percentile(err, 99)),

@@ -363,6 +363,14 @@ int quac_ensemble_run(quac_ensemble ens, double t0, double tmax, double dt0);
 int quac_ensemble_set_redo_margin(quac_ensemble ens, double margin);
 /* Steps of instance i re-evaluated in complex128 during the last run. */
 int64_t quac_ensemble_redone_steps(quac_ensemble ens, int64_t i);
+/* complex64 mode: every accepted step adds an estimate of the rounding its
+ * complex64 increments left in the state (8 eps32 h max_e sum_j |b_j dK_j|);
+ * once an instance's sum exceeds `budget` (default 1e-9) it takes its
+ * remaining steps with complex128 stages.  0 runs every step in complex128
+ * after the first. */
+int quac_ensemble_set_fp32_budget(quac_ensemble ens, double budget);
+/* Steps of instance i taken in complex128 after its budget ran out. */
+int64_t quac_ensemble_f64_steps(quac_ensemble ens, int64_t i);
 int quac_ensemble_get_stats(quac_ensemble ens, int64_t i, double *t, int64_t *steps, int64_t *rejected,
                             int *flags);
 /* Re(diag rho_i) of every instance, packed: D_0 values, then D_1, ... */

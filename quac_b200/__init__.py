@@ -206,6 +206,8 @@ def lib():
         "quac_ensemble_populations": (ctypes.c_int, [vp, vp]),
         "quac_ensemble_set_redo_margin": (ctypes.c_int, [vp, dbl]),
         "quac_ensemble_redone_steps": (i64, [vp, i64]),
+        "quac_ensemble_set_fp32_budget": (ctypes.c_int, [vp, dbl]),
+        "quac_ensemble_f64_steps": (i64, [vp, i64]),
         "create_op": (None, [ctypes.c_int, P(_OpPtr)]),
         "create_vec": (None, [ctypes.c_int, P(P(_OpPtr))]),
         "add_to_ham": (None, [Scalar, _OpPtr]),
@@ -886,6 +888,15 @@ class Ensemble:
 
     def redone_steps(self):
         return np.array([lib().quac_ensemble_redone_steps(self._h, i) for i in range(self.n)])
+
+    def set_fp32_budget(self, budget):
+        """complex64 mode: estimated accumulated complex64 error after which an
+        instance continues with complex128 stages (default 1e-9)."""
+        self._call("quac_ensemble_set_fp32_budget", float(budget))
+
+    def f64_steps(self):
+        """Per instance, the steps taken in complex128 after its budget ran out."""
+        return np.array([lib().quac_ensemble_f64_steps(self._h, i) for i in range(self.n)])
 
     def set_shape(self, warps, ctas_per_sm, elems_per_thread):
         self._call("quac_ensemble_set_shape", warps, ctas_per_sm, elems_per_thread)

@@ -82,6 +82,7 @@ struct EnsStatus {
   long long steps, rejected;
   int flags;   // 1: step limit reached, 2: non-finite error norm
   int redone;  // complex64 mode: steps whose estimate was taken again in complex128
+  int f64_steps;  // complex64 mode: steps taken in complex128 after the error budget ran out
 };
 
 struct EnsParams {
@@ -99,6 +100,7 @@ struct EnsParams {
   double t0, tmax, h0, atol, rtol, hmin, hmax;
   long long max_steps;
   double redo_margin;    // complex64 mode: |err - 1| below this re-evaluates the step in complex128
+  double f32_budget;     // complex64 mode: estimated accumulated complex64 error that switches an instance to complex128
 };
 
 __device__ __forceinline__ void cmac(double &ax, double &ay, double2 a, double2 b) {
@@ -184,6 +186,19 @@ __device__ double group_sum(double v, int gi, int gw, double *red) {
   return s;
 }
 
+__device__ double group_max(double v, int gi, int gw, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (gw == 1) return v;
+  const int w = (int)(threadIdx.x >> 5) - gi * gw;
+  if ((threadIdx.x & 31) == 0) red[gi * gw + w] = v;
+  group_sync(gi, gw);
+  double s = 0.0;
+  for (int k = 0; k < gw; k++) s = fmax(s, red[gi * gw + k]);
+  group_sync(gi, gw);
+  return s;
+}
+
 __device__ __forceinline__ double2 axpy(double2 y, double a, double2 x) {
   return make_double2(fma(a, x.x, y.x), fma(a, x.y, y.y));
 }
@@ -262,8 +277,12 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
   float2 *const Kb32 = (float2 *)Kb64;                      // dK_{j+2} at Kb32 + j C
   int iy = 0;
   double t = P.t0, h = P.h0;
-  long long steps = 0, rej = 0, redo = 0;
+  long long steps = 0, rej = 0, redo = 0, f64_steps = 0;
   int flags = 0;
+  // complex64 mode: estimated complex64 error accumulated by the accepted
+  // steps; past P.f32_budget the instance continues in complex128
+  double e32 = 0.0, dk_step = 0.0;
+  bool all64 = MODE == 0;
   const double tend_tol = 1e-12 * fmax(1.0, fabs(P.tmax));
   double bsum = 0.0;
   for (int j = 0; j < 6; j++) bsum += eA[6][j];
@@ -348,7 +367,7 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
     group_sync(gi, gw);
     eval64_into(K7);
     // error norm: h sum_j e_j K_j, weighted RMS (own elements only: no barrier needed)
-    double loc = 0.0;
+    double loc = 0.0, dkloc = 0.0;
     for (ElemIt it(lt, gt, D); it.ok(); it.next()) {
       double2 er;
       if (f64) {
@@ -359,14 +378,25 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
         // sum_j e_j = 0, so sum_j e_j K_j = sum_{j=2..6} e_j dK_j + e_7 (K7 - K1)
         const double2 k1 = K1[it.e], k7 = K7[it.e];
         er = make_double2(ht * eE[6] * (k7.x - k1.x), ht * eE[6] * (k7.y - k1.y));
-        for (int j = 1; j < 6; j++) er = axpy(er, ht * eE[j], Kb32[(size_t)(j - 1) * C + it.e]);
+        double dk = 0.0;
+        for (int j = 1; j < 6; j++) {
+          const float2 d = Kb32[(size_t)(j - 1) * C + it.e];
+          er = axpy(er, ht * eE[j], d);
+          dk += fabs(eA[6][j]) * (fabs((double)d.x) + fabs((double)d.y));
+        }
+        dkloc = fmax(dkloc, dk);
       }
       const double2 a = y[it.e], b = y5[it.e];
       const double m = fmax(sqrt(a.x * a.x + a.y * a.y), sqrt(b.x * b.x + b.y * b.y));
       const double q = sqrt(er.x * er.x + er.y * er.y) / (P.atol + P.rtol * m);
       loc += q * q;
     }
-    return sqrt(group_sum(loc, gi, gw, red) / (double)n);
+    const double en = sqrt(group_sum(loc, gi, gw, red) / (double)n);
+    // rounding of the complex64 increments in y5 = y + h sum_j b_j K_j:
+    // about eps32 |b_j dK_j| per element and stage, with a factor 8 for
+    // the complex64 sums inside each dK_j
+    if (!f64) dk_step = 8.0 * 5.96e-8 * ht * group_max(dkloc, gi, gw, red);
+    return en;
   };
 
   while (t < P.tmax - tend_tol) {
@@ -376,12 +406,14 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
     if (t + ht >= P.tmax - tend_tol) { ht = P.tmax - t; last = true; }
     const double2 *y = iy ? yb : ys;
     double2 *y5 = iy ? ys : yb;
-    double err = attempt(MODE == 0, ht, y, y5);
+    dk_step = 0.0;
+    double err = attempt(all64, ht, y, y5);
     // MODE 1: an estimate near the accept threshold is taken again with
     // complex128 stages, so accept / reject follows the complex128 decision
-    if (MODE == 1 && isfinite(err) && fabs(err - 1.0) < P.redo_margin) {
+    if (MODE == 1 && !all64 && isfinite(err) && fabs(err - 1.0) < P.redo_margin) {
       group_sync(gi, gw);
       err = attempt(true, ht, y, y5);
+      dk_step = 0.0;
       redo++;
     }
     if (!isfinite(err)) { flags |= 2; break; }
@@ -395,6 +427,11 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
       K7 = tmp;
       t = last ? P.tmax : t + ht;
       steps++;
+      if (MODE == 1) {
+        if (all64) f64_steps++;
+        e32 += dk_step;
+        if (!(e32 <= P.f32_budget)) all64 = true;
+      }
     } else {
       rej++;
     }
@@ -412,6 +449,7 @@ __device__ void integrate_instance(const EnsParams &P, const EnsInst &I, int gi,
     st.rejected = rej;
     st.flags = flags;
     st.redone = (int)redo;
+    st.f64_steps = (int)f64_steps;
     P.status[I.id] = st;
   }
 }
@@ -470,6 +508,7 @@ struct quac_ensemble_s {
   double atol = 5e-7, rtol = 5e-7, hmin = 0.01, hmax = 1.0;
   long long max_steps = 1000000;
   double redo_margin = 0.1;
+  double f32_budget = 1e-9;
   int warps = 16, cps = 1, ept = 8;  // launch shape
   // device
   unsigned char *d_tables = nullptr, *d_scratch = nullptr;
@@ -612,6 +651,7 @@ bool build_plan(quac_ensemble E) {
   p.hmax = E->hmax;
   p.max_steps = E->max_steps;
   p.redo_margin = E->redo_margin;
+  p.f32_budget = E->f32_budget;
   E->grid = grid;
   E->smem = (size_t)arena * E->warps;
   E->plan_valid = true;
@@ -810,6 +850,18 @@ int quac_ensemble_set_redo_margin(quac_ensemble E, double margin) {
   E->redo_margin = margin;
   E->plan_valid = false;
   return 0;
+}
+
+int quac_ensemble_set_fp32_budget(quac_ensemble E, double budget) {
+  if (!(budget >= 0.0)) { fail(0, "ERROR! ensemble complex64 error budget must be >= 0\n"); return 1; }
+  E->f32_budget = budget;
+  return 0;
+}
+
+int64_t quac_ensemble_f64_steps(quac_ensemble E, int64_t i) {
+  if (i < 0 || i >= E->n) { fail(0, "ERROR! ensemble index out of range\n"); return -1; }
+  if (!read_status(E)) return -1;
+  return E->status[i].f64_steps;
 }
 
 int64_t quac_ensemble_redone_steps(quac_ensemble E, int64_t i) {

@@ -145,6 +145,39 @@ def test_ensemble_fp32_rhs_within_1e8_of_oracle_at_tight_tolerance(quac, oracle,
     E.destroy()
 
 
+def test_ensemble_fp32_rhs_with_error_budget_within_1e8_at_default_tolerance(quac):
+    """complex64 increments at the default tolerance (5e-7) over the full
+    t = 100 run, 256 instances: an instance whose estimated accumulated
+    complex64 error passes the budget (1e-9) continues in complex128, so
+    every instance's populations stay within 1e-8 of the FP64 ensemble
+    (which the parity test above holds to the oracle); without the budget
+    some do not."""
+    params = Sy.driven_jc_ensemble_params(256, seed=4)
+    E, rho0 = _ensemble(quac, params)
+    E.set_options(precision=0)
+    E.set_states(rho0)
+    E.run(0.0, 100.0, DT0)
+    ref = E.get_states()
+    errs = {}
+    for budget in (1e-9, 1e30):
+        E.set_options(precision=1)
+        E.set_fp32_budget(budget)
+        E.set_states(rho0)
+        E.run(0.0, 100.0, DT0)
+        y = E.get_states()
+        errs[budget] = max(np.abs(E.state(ref, i).diagonal().real - E.state(y, i).diagonal().real).max()
+                           for i in range(len(params)))
+        if budget == 1e-9:
+            switched = int((E.f64_steps() > 0).sum())
+    print(f"population error vs FP64: budget 1e-9 {errs[1e-9]:.2e} ({switched} of 256 instances switched), "
+          f"no budget {errs[1e30]:.2e}")
+    assert errs[1e-9] <= 1e-8
+    assert errs[1e30] > errs[1e-9]
+    with pytest.raises(quac.QuacError):
+        E.set_fp32_budget(-1.0)
+    E.destroy()
+
+
 def test_ensemble_rejects_bad_input(quac):
     E, rho0 = _ensemble(quac, PARAMS[:2])
     with pytest.raises(quac.QuacError):

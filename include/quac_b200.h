@@ -365,7 +365,7 @@ int quac_ensemble_set_redo_margin(quac_ensemble ens, double margin);
 int64_t quac_ensemble_redone_steps(quac_ensemble ens, int64_t i);
 /* complex64 mode: every accepted step adds an estimate of the rounding its
  * complex64 increments left in the state (8 eps32 h max_e sum_j |b_j dK_j|);
- * once an instance's sum exceeds `budget` (default 1e-9) it takes its
+ * once an instance's sum exceeds `budget` (default 1e-7) it takes its
  * remaining steps with complex128 stages.  0 runs every step in complex128
  * after the first. */
 int quac_ensemble_set_fp32_budget(quac_ensemble ens, double budget);

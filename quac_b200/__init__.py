@@ -891,7 +891,7 @@ class Ensemble:
 
     def set_fp32_budget(self, budget):
         """complex64 mode: estimated accumulated complex64 error after which an
-        instance continues with complex128 stages (default 1e-9)."""
+        instance continues with complex128 stages (default 1e-7)."""
         self._call("quac_ensemble_set_fp32_budget", float(budget))
 
     def f64_steps(self):

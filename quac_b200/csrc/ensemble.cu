@@ -508,7 +508,7 @@ struct quac_ensemble_s {
   double atol = 5e-7, rtol = 5e-7, hmin = 0.01, hmax = 1.0;
   long long max_steps = 1000000;
   double redo_margin = 0.1;
-  double f32_budget = 1e-9;
+  double f32_budget = 1e-7;
   int warps = 16, cps = 1, ept = 8;  // launch shape
   // device
   unsigned char *d_tables = nullptr, *d_scratch = nullptr;

@@ -457,14 +457,11 @@ def steady_summary(q):
     Liouvillian (the method, from e0) and of the learned start with the
     preconditioned complex64-inner / complex128-refined solver; every solve
     to ||b - A x|| <= 1e-12 (tighter than the configuration's 1e-10, so
-    that the arms agree on populations to 1e-8).  Held-out points are
-    solved in blocks of 8 whose preconditioners are set up together (8
-    decompositions in flight on host threads), as a sweep would run."""
+    that the arms agree on populations to 1e-8)."""
     from quac_b200 import warmstart as WS
-    out = WS.measure_sweep(q, WS.sweep_settings(ne=6, nc=8, train=100, held=24, precond=1, cold_sample=1,
-                                                steps=4000, fp32=1, rtol=1e-12, block=8, threads=8))
-    return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "rtol", "block", "solver",
-                                "generation",
+    out = WS.measure_sweep(q, WS.sweep_settings(ne=6, nc=8, train=100, held=20, precond=1, cold_sample=1,
+                                                steps=4000, fp32=1, rtol=1e-12))
+    return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "rtol", "solver", "generation",
                                 "training",
                                 "cold", "method", "learned", "learned_vs_cold", "learned_vs_method",
                                 "method_vs_cold", "decompositions", "pop_err_max", "residual_max")}
@@ -612,8 +609,7 @@ def run_profile(args):
       --profile ensemble --instances N --t-end T [--fp32]          one persistent ensemble launch
       --profile gemm     --m M --n N --k K --reps R                 TF32 tensor-core GEMM
       --profile steady   --ne E --nc C --train T --held H --kd K --restart M --fp32-basis B --sweep2d
-                         --precond P --cold-sample S --train-steps N --block B --threads T
-                                                                       one steady-state sweep
+                         --precond P --cold-sample S --train-steps N   one steady-state sweep
                                                                      learned warm-start sweep
     """
     import ctypes
@@ -689,8 +685,7 @@ def run_profile(args):
         from quac_b200 import warmstart
         a = warmstart.sweep_settings(ne=args.ne, nc=args.nc, train=args.train, held=args.held, kd=args.kd,
                                      restart=args.restart, fp32=args.fp32_basis, sweep2d=args.sweep2d,
-                                     precond=args.precond, cold_sample=args.cold_sample, steps=args.train_steps,
-                                     block=args.block, threads=args.threads)
+                                     precond=args.precond, cold_sample=args.cold_sample, steps=args.train_steps)
         print(json.dumps(warmstart.measure_sweep(q, a)))
 
 
@@ -726,8 +721,6 @@ def main():
     ap.add_argument("--precond", type=int, default=1)
     ap.add_argument("--cold-sample", type=int, default=None)
     ap.add_argument("--train-steps", type=int, default=8000)
-    ap.add_argument("--block", type=int, default=0)
-    ap.add_argument("--threads", type=int, default=8)
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

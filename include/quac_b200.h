@@ -469,10 +469,6 @@ int quac_set_gmres_tolerance(double rtol);
  * way ahead of KSPSolve).  Builds qsys's steady-state preconditioner now;
  * 0 on success. */
 int quac_steady_precond_setup(qsystem qsys);
-/* Builds the preconditioners of n systems with up to nthreads
- * eigen-decompositions in flight at once (own host thread, solver handle
- * and stream each): the setup of a parameter sweep's next points. */
-int quac_steady_precond_setup_many(qsystem *systems, int n, int nthreads);
 /* Decompositions computed in this process and their total host time (s). */
 void quac_steady_precond_stats(int64_t *builds, double *seconds);
 /* Restart length of the steady-state GMRES (default 100 as in solver.c;

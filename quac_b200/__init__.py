@@ -170,7 +170,6 @@ def lib():
         "quac_set_gmres_preconditioner": (ctypes.c_int, [ctypes.c_int]),
         "quac_steady_precond_setup": (ctypes.c_int, [P(_QsysStruct)]),
         "quac_set_gmres_tolerance": (ctypes.c_int, [dbl]),
-        "quac_steady_precond_setup_many": (ctypes.c_int, [P(P(_QsysStruct)), ctypes.c_int, ctypes.c_int]),
         "quac_steady_precond_stats": (None, [ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
         "quac_set_gmres_restart": (ctypes.c_int, [ctypes.c_int]),
         "quac_set_gmres_precision": (ctypes.c_int, [ctypes.c_int]),
@@ -824,14 +823,6 @@ def steady_precond_setup(qs):
     """Builds qs's steady-state preconditioner now (eigen-decomposition of
     H_eff on the GPU)."""
     lib().quac_steady_precond_setup(qs._ptr)
-    _check()
-
-
-def steady_precond_setup_many(systems, nthreads=8):
-    """Builds the preconditioners of several systems with up to nthreads
-    decompositions in flight at once."""
-    arr = (ctypes.POINTER(_QsysStruct) * len(systems))(*[qs._ptr for qs in systems])
-    lib().quac_steady_precond_setup_many(arr, len(systems), int(nthreads))
     _check()
 
 

@@ -18,7 +18,6 @@
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
-#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -26,8 +25,6 @@
 #include <map>
 #include <memory>
 #include <mutex>
-#include <string>
-#include <thread>
 #include <vector>
 
 #include "runtime.h"
@@ -124,124 +121,87 @@ bool ensure_scratch(DeviceCtx &C, size_t n2) {
   return true;
 }
 
-// dense H_eff of qs, column-major (host only)
-bool dense_heff(qsystem qs, std::vector<std::complex<double>> &H, int &D) {
+// eigen-decomposition of H_eff of qs (caller holds g_mu); nullptr on failure
+std::shared_ptr<Decomp> decompose(qsystem qs, DeviceCtx &C, cudaStream_t s) {
+  const auto t0 = std::chrono::steady_clock::now();
   HostProg hp;
-  if (!compile_host(qs, 2, hp)) return false;  // -i H_eff in Schroedinger form
-  D = hp.D;
+  if (!compile_host(qs, 2, hp)) return nullptr;  // -i H_eff in Schroedinger form
+  const int D = hp.D;
   const size_t n2 = (size_t)D * D;
-  H.assign(n2, 0.0);
-  const std::complex<double> I(0.0, 1.0);  // H_eff = i (-i H_eff)
+  // dense H_eff, column-major: H_eff = i (-i H_eff)
+  std::vector<std::complex<double>> H(n2, 0.0);
+  const std::complex<double> I(0.0, 1.0);
   for (int r = 0; r < D; r++) H[(size_t)r * D + r] += I * hp.dr[r];
   for (size_t t = 0; t < hp.Lmap.size(); t++)
     for (int r = 0; r < D; r++) {
       const int c = hp.Lmap[t][r];
       if (c >= 0) H[(size_t)c * D + r] += I * hp.Lval[t][r];
     }
-  return true;
-}
-
-// V, V^-1 and the eigenvalues of the dense H (D x D) on stream s with the
-// given solver handle.  Touches no global state, so several run at once on
-// separate host threads; nullptr with err set on failure.
-std::shared_ptr<Decomp> decompose_dense(const std::vector<std::complex<double>> &H, int D, cusolverDnHandle_t sol,
-                                        cusolverDnParams_t par, cudaStream_t s, std::string &err) {
-  const size_t n2 = (size_t)D * D;
   auto P = std::make_shared<Decomp>();
   P->D = D;
+  QCUDA(cudaGetDevice(&P->device));
   double2 *A = nullptr;
   int64_t *ipiv = nullptr;
   int *info = nullptr;
   void *dwork = nullptr;
-  char msg[160];
-  auto cu = [&](cudaError_t e, const char *what) {
-    if (e == cudaSuccess) return true;
-    if (err.empty()) {
-      snprintf(msg, sizeof msg, "ERROR! %s failed in the preconditioner setup: %s\n", what, cudaGetErrorString(e));
-      err = msg;
-    }
-    return false;
-  };
-  auto so = [&](cusolverStatus_t st, const char *what) {
-    if (st == CUSOLVER_STATUS_SUCCESS) return true;
-    if (err.empty()) {
-      snprintf(msg, sizeof msg, "ERROR! %s failed (cuSOLVER status %d)\n", what, (int)st);
-      err = msg;
-    }
-    return false;
-  };
-  bool ok = cu(cudaGetDevice(&P->device), "cudaGetDevice") &&
-            cu(cudaMalloc(&P->V, n2 * sizeof(double2)), "cudaMalloc") &&
-            cu(cudaMalloc(&P->Vi, n2 * sizeof(double2)), "cudaMalloc") &&
-            cu(cudaMalloc(&P->lam, D * sizeof(double2)), "cudaMalloc") && cu(cudaMalloc(&A, n2 * sizeof(double2)), "cudaMalloc") &&
-            cu(cudaMalloc(&ipiv, D * sizeof(int64_t)), "cudaMalloc") && cu(cudaMalloc(&info, sizeof(int)), "cudaMalloc");
-  ok = ok && cu(cudaMemcpyAsync(A, H.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s), "copy of H_eff") &&
-       so(cusolverDnSetStream(sol, s), "cusolverDnSetStream");
+  QCUDA(cudaMalloc(&P->V, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&P->Vi, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&P->lam, D * sizeof(double2)));
+  QCUDA(cudaMalloc(&A, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&ipiv, D * sizeof(int64_t)));
+  QCUDA(cudaMalloc(&info, sizeof(int)));
+  bool ok = !has_error() && ensure_scratch(C, n2);
+  if (ok) QCUDA(cudaMemcpyAsync(A, H.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ok = ok && solver_ok(cusolverDnSetStream(C.sol, s), "cusolverDnSetStream");
   size_t dsz = 0, hsz = 0, dsz2 = 0, hsz2 = 0;
-  ok = ok &&
-       so(cusolverDnXgeev_bufferSize(sol, par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D, CUDA_C_64F, A,
-                                     D, CUDA_C_64F, P->lam, CUDA_C_64F, nullptr, D, CUDA_C_64F, P->V, D, CUDA_C_64F,
-                                     &dsz, &hsz),
-          "geev buffer size") &&
-       so(cusolverDnXgetrf_bufferSize(sol, par, D, D, CUDA_C_64F, P->Vi, D, CUDA_C_64F, &dsz2, &hsz2),
-          "getrf buffer size");
+  if (ok)
+    ok = solver_ok(cusolverDnXgeev_bufferSize(C.sol, C.par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D,
+                                              CUDA_C_64F, A, D, CUDA_C_64F, P->lam, CUDA_C_64F, nullptr, D,
+                                              CUDA_C_64F, P->V, D, CUDA_C_64F, &dsz, &hsz),
+                   "geev buffer size") &&
+         solver_ok(cusolverDnXgetrf_bufferSize(C.sol, C.par, D, D, CUDA_C_64F, P->Vi, D, CUDA_C_64F, &dsz2, &hsz2),
+                   "getrf buffer size");
   std::vector<char> hwork(std::max(hsz, hsz2) + 1);
-  ok = ok && cu(cudaMalloc(&dwork, std::max(dsz, dsz2) + 16), "cudaMalloc");
+  if (ok) QCUDA(cudaMalloc(&dwork, std::max(dsz, dsz2) + 16));
   int hinfo = 0;
-  ok = ok && so(cusolverDnXgeev(sol, par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D, CUDA_C_64F, A, D,
-                                CUDA_C_64F, P->lam, CUDA_C_64F, nullptr, D, CUDA_C_64F, P->V, D, CUDA_C_64F, dwork, dsz,
-                                hwork.data(), hsz, info),
-                "geev");
-  ok = ok && cu(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s), "copy of info") &&
-       cu(cudaStreamSynchronize(s), "geev");
-  if (ok && hinfo != 0) {
-    snprintf(msg, sizeof msg, "ERROR! eigen-decomposition of H_eff failed (info %d)\n", hinfo);
-    err = msg;
-    ok = false;
+  if (ok && !has_error())
+    ok = solver_ok(cusolverDnXgeev(C.sol, C.par, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, D, CUDA_C_64F,
+                                   A, D, CUDA_C_64F, P->lam, CUDA_C_64F, nullptr, D, CUDA_C_64F, P->V, D, CUDA_C_64F,
+                                   dwork, dsz, hwork.data(), hsz, info),
+                   "geev");
+  if (ok) {
+    QCUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    QCUDA(cudaStreamSynchronize(s));
+    if (hinfo != 0) { fail(9, "ERROR! eigen-decomposition of H_eff failed (info %d)\n", hinfo); ok = false; }
   }
   // V^-1: LU of V (in A), then solve with the identity on the right (in Vi)
-  std::vector<std::complex<double>> Id;
   if (ok) {
-    Id.assign(n2, 0.0);
+    std::vector<std::complex<double>> Id(n2, 0.0);
     for (int k = 0; k < D; k++) Id[(size_t)k * D + k] = 1.0;
-  }
-  ok = ok && cu(cudaMemcpyAsync(A, P->V, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, s), "copy of V") &&
-       cu(cudaMemcpyAsync(P->Vi, Id.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s), "copy of I") &&
-       so(cusolverDnXgetrf(sol, par, D, D, CUDA_C_64F, A, D, ipiv, CUDA_C_64F, dwork, dsz2, hwork.data(), hsz2, info),
-          "getrf") &&
-       so(cusolverDnXgetrs(sol, par, CUBLAS_OP_N, D, D, CUDA_C_64F, A, D, ipiv, CUDA_C_64F, P->Vi, D, info), "getrs") &&
-       cu(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s), "copy of info") &&
-       cu(cudaStreamSynchronize(s), "getrs");  // also keeps Id alive until its copy is done
-  if (ok && hinfo != 0) {
-    snprintf(msg, sizeof msg, "ERROR! eigenvector matrix of H_eff is singular (info %d)\n", hinfo);
-    err = msg;
-    ok = false;
+    QCUDA(cudaMemcpyAsync(A, P->V, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    QCUDA(cudaMemcpyAsync(P->Vi, Id.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ok = solver_ok(cusolverDnXgetrf(C.sol, C.par, D, D, CUDA_C_64F, A, D, ipiv, CUDA_C_64F, dwork, dsz2,
+                                    hwork.data(), hsz2, info),
+                   "getrf") &&
+         solver_ok(cusolverDnXgetrs(C.sol, C.par, CUBLAS_OP_N, D, D, CUDA_C_64F, A, D, ipiv, CUDA_C_64F, P->Vi, D,
+                                    info),
+                   "getrs");
+    if (ok) {
+      QCUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+      QCUDA(cudaStreamSynchronize(s));  // also keeps Id alive until the copy is done
+      if (hinfo != 0) { fail(9, "ERROR! eigenvector matrix of H_eff is singular (info %d)\n", hinfo); ok = false; }
+    }
   }
   if (ok) {
     std::vector<std::complex<double>> lam(D);
-    ok = cu(cudaMemcpy(lam.data(), P->lam, D * sizeof(double2), cudaMemcpyDeviceToHost), "copy of eigenvalues");
+    QCUDA(cudaMemcpy(lam.data(), P->lam, D * sizeof(double2), cudaMemcpyDeviceToHost));
     double scale = 0.0;
     for (auto &l : lam) scale = std::max(scale, std::abs(l));
     P->shift = 1e-8 * std::max(scale, 1e-300);  // modes without decay
   }
   for (void *p : {(void *)A, (void *)ipiv, (void *)info, dwork})
     if (p) cudaFree(p);
-  return ok ? P : nullptr;
-}
-
-// eigen-decomposition of H_eff of qs (caller holds g_mu); nullptr on failure
-std::shared_ptr<Decomp> decompose(qsystem qs, DeviceCtx &C, cudaStream_t s) {
-  const auto t0 = std::chrono::steady_clock::now();
-  std::vector<std::complex<double>> H;
-  int D = 0;
-  if (!dense_heff(qs, H, D)) return nullptr;
-  if (!ensure_scratch(C, (size_t)D * D)) return nullptr;
-  std::string err;
-  auto P = decompose_dense(H, D, C.sol, C.par, s, err);
-  if (!P) {
-    fail(9, "%s", err.c_str());
-    return nullptr;
-  }
+  if (!ok || has_error()) return nullptr;
   g_builds++;
   g_build_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return P;
@@ -314,87 +274,6 @@ extern "C" int quac_steady_precond_setup(qsystem qs) {
   if (!qs->mat_allocated) construct_matrix(qs);
   if (has_error()) return 1;
   return entry_for(qs, stream_of(qs)) ? 0 : 1;
-}
-
-// Builds the preconditioners of n systems with up to nthreads
-// decompositions in flight at once (each on its own host thread, solver
-// handle and stream).  A decomposition at D = 512 is thousands of small
-// kernels and host work, leaving the GPU mostly idle, so a parameter sweep
-// prepares the next points' preconditioners together.  The term programs
-// and the dense H_eff are built on the calling thread first.
-extern "C" int quac_steady_precond_setup_many(qsystem *systems, int n, int nthreads) {
-  if (n < 0 || nthreads < 1) { fail(0, "ERROR! preconditioner setup needs n >= 0 and nthreads >= 1\n"); return 1; }
-  std::lock_guard<std::mutex> lk(g_mu);
-  const auto t0 = std::chrono::steady_clock::now();
-  DeviceCtx *C = device_ctx();
-  if (!C) return 1;
-  struct Job {
-    qsystem qs;
-    uint64_t serial;
-    int D;
-    std::vector<std::complex<double>> H;
-    std::shared_ptr<Decomp> out;
-    std::string err;
-  };
-  std::vector<Job> jobs;
-  size_t maxn2 = 0;
-  for (int k = 0; k < n; k++) {
-    qsystem qs = systems[k];
-    if (!qs->mat_allocated) construct_matrix(qs);
-    ensure_program(qs);
-    if (has_error() || !qs->impl->prog) return 1;
-    SteadyPrecond &P = g_pre[qs];
-    P.ctx = C;
-    if (P.serial == qs->impl->prog->serial && P.dec) continue;
-    Job j;
-    j.qs = qs;
-    j.serial = qs->impl->prog->serial;
-    if (!dense_heff(qs, j.H, j.D)) return 1;
-    maxn2 = std::max(maxn2, (size_t)j.D * j.D);
-    jobs.push_back(std::move(j));
-  }
-  if (!ensure_scratch(*C, maxn2)) return 1;
-  int dev = 0;
-  QCUDA(cudaGetDevice(&dev));
-  std::atomic<size_t> next{0};
-  auto worker = [&]() {
-    cudaSetDevice(dev);
-    cusolverDnHandle_t sol = nullptr;
-    cusolverDnParams_t par = nullptr;
-    cudaStream_t st = nullptr;
-    std::string setup_err;
-    if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS || cusolverDnCreateParams(&par) != CUSOLVER_STATUS_SUCCESS ||
-        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
-      setup_err = "ERROR! preconditioner setup could not create its solver handle or stream\n";
-    for (size_t k; (k = next.fetch_add(1)) < jobs.size();) {
-      if (!setup_err.empty()) { jobs[k].err = setup_err; continue; }
-      jobs[k].out = decompose_dense(jobs[k].H, jobs[k].D, sol, par, st, jobs[k].err);
-    }
-    if (par) cusolverDnDestroyParams(par);
-    if (sol) cusolverDnDestroy(sol);
-    if (st) cudaStreamDestroy(st);
-  };
-  const int nt = (int)std::min<size_t>((size_t)nthreads, jobs.size());
-  std::vector<std::thread> pool;
-  for (int t = 1; t < nt; t++) pool.emplace_back(worker);
-  if (nt > 0) worker();
-  for (auto &th : pool) th.join();
-  int rc = 0;
-  int built = 0;
-  for (auto &j : jobs) {
-    if (!j.out) {
-      if (!rc) fail(9, "%s", j.err.empty() ? "ERROR! preconditioner setup failed\n" : j.err.c_str());
-      rc = 1;
-      continue;
-    }
-    SteadyPrecond &P = g_pre[j.qs];
-    P.dec = j.out;
-    P.serial = j.serial;
-    built++;
-  }
-  g_builds += built;
-  g_build_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  return rc;
 }
 
 // Decompositions computed in this process and their total host wall time.

@@ -153,13 +153,10 @@ def sweep_settings(**kw):
     """Settings of measure_sweep: ne emitters, nc cavity levels, train / held
     parameter points, 2-D sweep (kappa and gamma fixed), network training
     steps and learning rate, guided-solver basis precision (fp32), deflation
-    rank kd, restart length and refresh, preconditioner, cold sample size,
-    GMRES tolerance, and (preconditioned flow) the block of held-out points
-    whose preconditioners are set up together on `threads` host threads
-    (0: one point at a time); kw overrides the defaults."""
+    rank kd, restart length and refresh, preconditioner, cold sample size
+    and GMRES tolerance; kw overrides the defaults."""
     a = argparse.Namespace(ne=3, nc=4, train=48, held=12, sweep2d=False, steps=8000, lr=2e-3, fp32=1, kd=8,
-                           seed=5, restart=100, refresh=1, precond=0, cold_sample=None, rtol=1e-11,
-                           block=0, threads=8)
+                           seed=5, restart=100, refresh=1, precond=0, cold_sample=None, rtol=1e-11)
     for k, v in kw.items():
         setattr(a, k, v)
     return a
@@ -254,66 +251,17 @@ def measure_sweep(q, a):
     finish(arm_learned(train[0]))
 
     builds1 = q.steady_precond_stats()
-    def arm_block(ths, learned):
-        """The points of one block solved together: systems built first
-        (untimed, as in the per-point arms), then the timed region holds the
-        preconditioner setup of the whole block (a.threads decompositions in
-        flight), the network's proposals for the block, the upload of the
-        starts and the solves."""
-        if learned:
-            learned_settings()
-        else:
-            method_settings()
-        built = [WS.build_tc(q, th, a.ne, a.nc) for th in ths]
-        vecs = [q.create_qvec_sys(B.qs) for B in built]
-        t0 = time.perf_counter()
-        q.steady_precond_setup_many([B.qs for B in built], a.threads)
-        if learned:
-            F = net.predict(WS.normalize(np.asarray(ths)))
-            starts = [WS.proposal_from_factors(F[k], kd) for k in range(len(ths))]
-        else:
-            starts = [(e0, U0)] * len(ths)
-        out = []
-        for B, v, (x0, U) in zip(built, vecs, starts):
-            v.from_numpy(x0)
-            its, r_ = q.steady_state_guided(B.qs, v, U)
-            out.append((v.to_numpy(), its, r_))
-        dt = time.perf_counter() - t0
-        for B, v in zip(built, vecs):
-            v.destroy()
-            B.qs.destroy()
-        return out, dt
-
     rows = []
-    if a.precond and a.block > 1:
-        for k0 in range(0, len(held), a.block):
-            blk = held[k0:k0 + a.block]
-            cold = []
-            for k, th in enumerate(blk):
-                if k0 + k < ncold:
-                    plain_settings()
-                    cold.append(WS.solve_cold(q, th, a.ne, a.nc))
-                else:
-                    cold.append((None, -1, float("nan")))
-            om, dtm = arm_block(blk, False)
-            ol, dtl = arm_block(blk, True)
-            for k in range(len(blk)):
-                xc, its_c, dt_c = cold[k]
-                (xm, its_m, res_m), (xl, its_l, res_l) = om[k], ol[k]
-                pc = (xc if xc is not None else xm).reshape(D, D, order="F").diagonal().real
-                perr = max(np.abs(x.reshape(D, D, order="F").diagonal().real - pc).max() for x in (xm, xl))
-                rows.append((its_c, dt_c, its_m, dtm / len(blk), its_l, dtl / len(blk), perr, max(res_m, res_l)))
-    else:
-        for k, th in enumerate(held):
-            xc, its_c, dt_c = None, -1, float("nan")
-            if k < ncold:
-                plain_settings()
-                xc, its_c, dt_c = WS.solve_cold(q, th, a.ne, a.nc)
-            xm, its_m, res_m, dt_m = finish(arm_method(th))
-            xl, its_l, res_l, dt_l = finish(arm_learned(th))
-            pc = (xc if xc is not None else xm).reshape(D, D, order="F").diagonal().real
-            perr = max(np.abs(x.reshape(D, D, order="F").diagonal().real - pc).max() for x in (xm, xl))
-            rows.append((its_c, dt_c, its_m, dt_m, its_l, dt_l, perr, max(res_m, res_l)))
+    for k, th in enumerate(held):
+        xc, its_c, dt_c = None, -1, float("nan")
+        if k < ncold:
+            plain_settings()
+            xc, its_c, dt_c = WS.solve_cold(q, th, a.ne, a.nc)
+        xm, its_m, res_m, dt_m = finish(arm_method(th))
+        xl, its_l, res_l, dt_l = finish(arm_learned(th))
+        pc = (xc if xc is not None else xm).reshape(D, D, order="F").diagonal().real
+        perr = max(np.abs(x.reshape(D, D, order="F").diagonal().real - pc).max() for x in (xm, xl))
+        rows.append((its_c, dt_c, its_m, dt_m, its_l, dt_l, perr, max(res_m, res_l)))
     builds2 = q.steady_precond_stats()
     plain_settings()
     q.set_gmres_preconditioner(1)
@@ -326,7 +274,6 @@ def measure_sweep(q, a):
         "workload": f"tavis_cummings_steady_ne{a.ne}_nc{a.nc}_D{D}",
         "sweep": "2d (omega, delta)" if a.sweep2d else "4d (omega, delta, kappa, gamma)",
         "train_states": a.train, "held_out": n, "kd": kd, "rtol": a.rtol,
-        "block": ({"points": a.block, "threads": a.threads} if a.precond and a.block > 1 else None),
         "solver": ("GMRES(100) preconditioned by the exact inverse of the no-jump Liouvillian, "
                    + ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + " basis in the learned arm"
                    if a.precond else

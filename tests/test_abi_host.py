@@ -166,11 +166,6 @@ def test_error_mode_returns_instead_of_exiting(quac):
     qs.destroy()
 
 
-def test_precond_setup_many_validates_on_the_host(quac):
-    with pytest.raises(quac.QuacError):
-        quac.steady_precond_setup_many([], 0)
-
-
 def test_solver_option_setters_validate_on_the_host(quac):
     """The steady-state and L.x option setters check their arguments before
     touching any device state; each rejected value leaves the option as it

@@ -333,37 +333,3 @@ def test_preconditioned_flow(quac):
     assert out["decompositions"]["held_out"] == 12
     assert sum(out["learned"]["iterations"]) <= 2 * sum(out["method"]["iterations"])
     assert 5 * max(out["method"]["iterations"][:2]) < min(out["cold"]["iterations"])
-
-
-def test_precond_setup_many_matches_single_setup(quac):
-    """Preconditioners of several sweep points built together (four host
-    threads, decompositions in flight at once) give the same solves as the
-    one-at-a-time setup: same iteration counts and residual bar, and one
-    decomposition per system."""
-    from quac_b200 import warmstart as WS
-    ne, nc = 3, 4
-    D = 2 ** ne * nc
-    thetas = WS.sweep_params(6, seed=9)
-    e0 = np.zeros(D * D, complex)
-    e0[0] = 1.0
-    single = []
-    for th in thetas:
-        B, v, its, res, _ = WS.solve_guided(quac, th, ne, nc, e0, np.eye(D, 0, dtype=complex))
-        single.append((its, v.to_numpy()))
-        v.destroy()
-        B.qs.destroy()
-    built = [WS.build_tc(quac, th, ne, nc) for th in thetas]
-    n0 = quac.steady_precond_stats()[0]
-    quac.steady_precond_setup_many([B.qs for B in built], 4)
-    assert quac.steady_precond_stats()[0] - n0 == len(thetas)
-    quac.steady_precond_setup_many([B.qs for B in built], 4)  # cached: nothing rebuilt
-    assert quac.steady_precond_stats()[0] - n0 == len(thetas)
-    for B, (its1, x1) in zip(built, single):
-        v = quac.create_qvec_sys(B.qs)
-        v.from_numpy(e0)
-        its, res = quac.steady_state_guided(B.qs, v, np.eye(D, 0, dtype=complex))
-        assert res <= 1e-11
-        assert abs(its - its1) <= 2
-        assert np.abs(v.to_numpy() - x1).max() < 1e-9
-        v.destroy()
-        B.qs.destroy()

@@ -459,7 +459,7 @@ def steady_summary(q):
     to ||b - A x|| <= 1e-12 (tighter than the configuration's 1e-10, so
     that the arms agree on populations to 1e-8)."""
     from quac_b200 import warmstart as WS
-    out = WS.measure_sweep(q, WS.sweep_settings(ne=6, nc=8, train=100, held=20, precond=1, cold_sample=1,
+    out = WS.measure_sweep(q, WS.sweep_settings(ne=6, nc=8, train=100, held=20, precond=2, cold_sample=1,
                                                 steps=4000, fp32=1, rtol=1e-12))
     return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "rtol", "solver", "generation",
                                 "training",

@@ -455,11 +455,15 @@ int quac_set_lrho_precision(int precision);
  * Hermitian to 1e-13; 0 = always compute every element. */
 int quac_set_hermitian_mode(int mode);
 /* Preconditioner of the steady-state GMRES (the role PCASM / ILU(0) plays in
- * solver.c:167-198): 1 (default) = the exact inverse of the no-jump
+ * solver.c:167-198): 1 = the exact inverse of the no-jump
  * Liouvillian L0 X = -i (H_eff X - X H_eff^H), H_eff = H - i/2 sum a C^dag C,
  * applied on the right through the eigen-decomposition of H_eff (computed
  * once per system on the GPU; four D x D complex GEMMs per iteration);
- * 0 = none.  The guided solve with a deflation space runs unpreconditioned. */
+ * 2 (default) = the same form built from the Hermitian eigensolver: H_eff = H - i/2 G,
+ * H = U diag(w) U^H, eigenvalues of H_eff taken as w_k - i/2 (U^H G U)_kk
+ * (exact when G commutes with H, a fixed approximation otherwise; cheaper to
+ * set up, GMRES still converges to the same answer); 0 = none.  The guided
+ * solve with a deflation space runs unpreconditioned. */
 int quac_set_gmres_preconditioner(int mode);
 /* Tolerance of the steady-state GMRES on the true residual ||b - A x||
  * with ||b|| = 1 (default 1e-11 as solver.c:14, 179; -ksp_rtol on the

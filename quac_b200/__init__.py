@@ -807,8 +807,10 @@ def set_deflation_refresh(mode):
 
 
 def set_gmres_preconditioner(mode):
-    """1 (default): steady-state GMRES preconditioned by the exact inverse of
-    the no-jump Liouvillian; 0: none."""
+    """2 (default): steady-state GMRES preconditioned by the inverse of the
+    no-jump Liouvillian built from the Hermitian part of H_eff (approximate,
+    cheap setup); 1: its exact inverse (non-Hermitian eigen-decomposition);
+    0: none."""
     lib().quac_set_gmres_preconditioner(int(mode))
     _check()
 

@@ -1443,7 +1443,10 @@ extern "C" int quac_set_gmres_tolerance(double rtol) {
 }
 
 extern "C" int quac_set_gmres_preconditioner(int mode) {
-  if (mode != 0 && mode != 1) { fail(0, "ERROR! GMRES preconditioner must be 0 (none) or 1 (no-jump inverse)\n"); return 1; }
+  if (mode < 0 || mode > 2) {
+    fail(0, "ERROR! GMRES preconditioner must be 0 (none), 1 (no-jump inverse) or 2 (its Hermitian-part form)\n");
+    return 1;
+  }
   options().gmres_precond = mode;
   return 0;
 }

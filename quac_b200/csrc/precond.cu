@@ -36,6 +36,7 @@ bool compile_host(qsystem qs, int mode, HostProg &hp);
 // V, V^-1 and the eigenvalues of one H_eff (device memory)
 struct Decomp {
   int D = 0;
+  int kind = 1;  // 1: eigen-decomposition of H_eff; 2: of its Hermitian part
   int device = 0;
   double shift = 0.0;
   double2 *V = nullptr, *Vi = nullptr, *lam = nullptr;
@@ -76,6 +77,25 @@ __global__ void k_sylvester_scale(double2 *__restrict__ y, const double2 *__rest
     const double2 v = y[i];
     y[i] = make_double2((v.x * dr + v.y * di) * inv, (v.y * dr - v.x * di) * inv);
   }
+}
+
+// lam[k] = w[k] - i/2 Re(sum_i conj(U[i, k]) T[i, k]), T = G U (column-major)
+__global__ void k_herm_eigs(const double2 *__restrict__ U, const double2 *__restrict__ T, const double *__restrict__ w,
+                            double2 *__restrict__ lam, int D) {
+  const int k = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < D; i += PT) {
+    const double2 u = U[(size_t)k * D + i], t = T[(size_t)k * D + i];
+    s += u.x * t.x + u.y * t.y;
+  }
+  __shared__ double red[PT];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = PT / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) lam[k] = make_double2(w[k], -0.5 * red[0]);
 }
 
 bool blas_ok(cublasStatus_t st, const char *what) {
@@ -121,6 +141,90 @@ bool ensure_scratch(DeviceCtx &C, size_t n2) {
   return true;
 }
 
+// Mode 2: H_eff = H - i/2 G with H, G Hermitian; H = U diag(w) U^H by the
+// Hermitian eigensolver, and the eigenvalues of H_eff approximated by
+// w_k - i/2 (U^H G U)_kk.  V = U is unitary (V^-1 = U^H), so the setup needs
+// no LU; the preconditioner is exact when G commutes with H and otherwise a
+// fixed approximation of L0^-1, which GMRES tolerates (it still minimises
+// the true residual).
+std::shared_ptr<Decomp> decompose_hermitian(int D, const std::vector<std::complex<double>> &Heff, DeviceCtx &C,
+                                            cudaStream_t s) {
+  const size_t n2 = (size_t)D * D;
+  std::vector<std::complex<double>> H(n2), G(n2);
+  const std::complex<double> I(0.0, 1.0);
+  for (int c = 0; c < D; c++)
+    for (int r = 0; r < D; r++) {
+      const std::complex<double> a = Heff[(size_t)c * D + r], b = std::conj(Heff[(size_t)r * D + c]);
+      H[(size_t)c * D + r] = 0.5 * (a + b);
+      G[(size_t)c * D + r] = I * (a - b);
+    }
+  auto P = std::make_shared<Decomp>();
+  P->D = D;
+  P->kind = 2;
+  QCUDA(cudaGetDevice(&P->device));
+  double2 *Gd = nullptr, *T = nullptr;
+  double *w = nullptr;
+  int *info = nullptr;
+  void *dwork = nullptr;
+  QCUDA(cudaMalloc(&P->V, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&P->Vi, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&P->lam, D * sizeof(double2)));
+  QCUDA(cudaMalloc(&Gd, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&T, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&w, D * sizeof(double)));
+  QCUDA(cudaMalloc(&info, sizeof(int)));
+  bool ok = !has_error();
+  if (ok) {
+    QCUDA(cudaMemcpyAsync(P->V, H.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
+    QCUDA(cudaMemcpyAsync(Gd, G.data(), n2 * sizeof(double2), cudaMemcpyHostToDevice, s));
+  }
+  ok = ok && !has_error() && solver_ok(cusolverDnSetStream(C.sol, s), "cusolverDnSetStream");
+  size_t dsz = 0, hsz = 0;
+  ok = ok && solver_ok(cusolverDnXsyevd_bufferSize(C.sol, C.par, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, D,
+                                                   CUDA_C_64F, P->V, D, CUDA_R_64F, w, CUDA_C_64F, &dsz, &hsz),
+                       "syevd buffer size");
+  std::vector<char> hwork(hsz + 1);
+  if (ok) QCUDA(cudaMalloc(&dwork, dsz + 16));
+  ok = ok && !has_error() &&
+       solver_ok(cusolverDnXsyevd(C.sol, C.par, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, D, CUDA_C_64F, P->V,
+                                  D, CUDA_R_64F, w, CUDA_C_64F, dwork, dsz, hwork.data(), hsz, info),
+                 "syevd");
+  int hinfo = 0;
+  if (ok) {
+    QCUDA(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    QCUDA(cudaStreamSynchronize(s));
+    if (hinfo != 0) { fail(9, "ERROR! eigen-decomposition of the Hermitian part of H_eff failed (info %d)\n", hinfo); ok = false; }
+  }
+  if (ok && !C.blas) ok = blas_ok(cublasCreate(&C.blas), "cublasCreate");
+  if (ok) {
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    auto *cU = reinterpret_cast<cuDoubleComplex *>(P->V);
+    ok = blas_ok(cublasSetStream(C.blas, s), "cublasSetStream") &&
+         blas_ok(cublasZgemm(C.blas, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one,
+                             reinterpret_cast<const cuDoubleComplex *>(Gd), D, cU, D, &zero,
+                             reinterpret_cast<cuDoubleComplex *>(T), D),
+                 "zgemm") &&
+         blas_ok(cublasZgeam(C.blas, CUBLAS_OP_C, CUBLAS_OP_N, D, D, &one, cU, D, &zero, cU, D,
+                             reinterpret_cast<cuDoubleComplex *>(P->Vi), D),
+                 "zgeam");
+  }
+  if (ok) {
+    k_herm_eigs<<<D, PT, 0, s>>>(P->V, T, w, P->lam, D);
+    count_launch();
+    QCUDA(cudaGetLastError());
+    std::vector<std::complex<double>> lam(D);
+    QCUDA(cudaMemcpyAsync(lam.data(), P->lam, D * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    QCUDA(cudaStreamSynchronize(s));
+    double scale = 0.0;
+    for (auto &l : lam) scale = std::max(scale, std::abs(l));
+    P->shift = 1e-8 * std::max(scale, 1e-300);
+  }
+  for (void *p : {(void *)Gd, (void *)T, (void *)w, (void *)info, dwork})
+    if (p) cudaFree(p);
+  if (!ok || has_error()) return nullptr;
+  return P;
+}
+
 // eigen-decomposition of H_eff of qs (caller holds g_mu); nullptr on failure
 std::shared_ptr<Decomp> decompose(qsystem qs, DeviceCtx &C, cudaStream_t s) {
   const auto t0 = std::chrono::steady_clock::now();
@@ -137,6 +241,14 @@ std::shared_ptr<Decomp> decompose(qsystem qs, DeviceCtx &C, cudaStream_t s) {
       const int c = hp.Lmap[t][r];
       if (c >= 0) H[(size_t)c * D + r] += I * hp.Lval[t][r];
     }
+  if (options().gmres_precond == 2) {
+    if (!ensure_scratch(C, n2)) return nullptr;
+    auto Q = decompose_hermitian(D, H, C, s);
+    if (!Q) return nullptr;
+    g_builds++;
+    g_build_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return Q;
+  }
   auto P = std::make_shared<Decomp>();
   P->D = D;
   QCUDA(cudaGetDevice(&P->device));
@@ -216,7 +328,8 @@ SteadyPrecond *entry_for(qsystem qs, cudaStream_t s) {
   SteadyPrecond &P = g_pre[qs];
   P.ctx = C;
   const uint64_t serial = qs->impl->prog->serial;
-  if (P.serial == serial && P.dec) return ensure_scratch(*C, (size_t)P.dec->D * P.dec->D) ? &P : nullptr;
+  if (P.serial == serial && P.dec && P.dec->kind == options().gmres_precond)
+    return ensure_scratch(*C, (size_t)P.dec->D * P.dec->D) ? &P : nullptr;
   P.dec.reset();
   P.serial = 0;
   auto d = decompose(qs, *C, s);

@@ -67,7 +67,7 @@ struct Options {
   int defl_refresh = 1;             // see quac_set_deflation_refresh
   double gmres_rtol = 1e-11;        // -ksp_rtol (solver.c:14, 179: 1e-11 on ||b|| = 1)
   int gmres_restart = 100;          // -ksp_gmres_restart (solver.c uses PETSc's default 100 via KSPGMRESSetRestart)
-  int gmres_precond = 1;            // see quac_set_gmres_preconditioner
+  int gmres_precond = 2;            // see quac_set_gmres_preconditioner
   bool rk4_classic = false;         // rk_type "4classic": four-stage form instead of Horner
 };
 Options &options();

@@ -10,12 +10,13 @@ kappa ~ U[0.01, 0.2], gamma ~ U[1e-3, 1e-2], g = 0.1):
    F F^H ~ rho_ss;
 3. a new point is solved from the proposal F F^H / tr.
 
-With the steady-state preconditioner on (quac_set_gmres_preconditioner,
-the exact inverse of the no-jump Liouvillian) every solve is a
-preconditioned GMRES(100) started from the better of the proposal and e0;
-the eigen-decomposition behind the preconditioner is most of such a solve
-at D = 512 and the proposal cannot shorten it.  With the preconditioner
-off, the proposal also supplies a deflation space
+With the steady-state preconditioner on (quac_set_gmres_preconditioner:
+the inverse of the no-jump Liouvillian, exact or from the Hermitian part of
+H_eff) every solve is a preconditioned GMRES(100) started from the better
+of the proposal and e0; the eigen-decomposition behind the preconditioner
+is a large part of such a solve at D = 512 and the proposal cannot shorten
+it.  With the preconditioner off, the proposal also supplies a deflation
+space
 { u_i u_j^H } from the kd leading left singular vectors of F
 (quac_steady_state_guided: Galerkin projection refreshed at every restart
 from the iterate), which is what makes unpreconditioned GMRES converge on
@@ -264,7 +265,7 @@ def measure_sweep(q, a):
         rows.append((its_c, dt_c, its_m, dt_m, its_l, dt_l, perr, max(res_m, res_l)))
     builds2 = q.steady_precond_stats()
     plain_settings()
-    q.set_gmres_preconditioner(1)
+    q.set_gmres_preconditioner(2)
     q.set_deflation_refresh(1)
     q.set_gmres_tolerance(1e-11)
     r = np.array(rows)
@@ -274,7 +275,9 @@ def measure_sweep(q, a):
         "workload": f"tavis_cummings_steady_ne{a.ne}_nc{a.nc}_D{D}",
         "sweep": "2d (omega, delta)" if a.sweep2d else "4d (omega, delta, kappa, gamma)",
         "train_states": a.train, "held_out": n, "kd": kd, "rtol": a.rtol,
-        "solver": ("GMRES(100) preconditioned by the exact inverse of the no-jump Liouvillian, "
+        "solver": ("GMRES(100) preconditioned by the "
+                   + ("exact inverse" if a.precond == 1 else "Hermitian-part form of the inverse")
+                   + " of the no-jump Liouvillian, "
                    + ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + " basis in the learned arm"
                    if a.precond else
                    ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + f" GMRES({a.restart})"

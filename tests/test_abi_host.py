@@ -175,7 +175,7 @@ def test_solver_option_setters_validate_on_the_host(quac):
                               (q.set_deflation_refresh, (0, 1), (2,)),
                               (q.set_gmres_restart, (300, 1024, 100), (0, 1025)),
                               (q.set_hermitian_mode, (0, 1), (3,)),
-                              (q.set_gmres_preconditioner, (0, 1), (2, -1)),
+                              (q.set_gmres_preconditioner, (0, 2, 1), (3, -1)),
                               (q.set_gmres_tolerance, (1e-12, 1e-11), (0.0, -1e-3, 1.0)),
                               (q.set_lrho_precision, (1, 0), (2,))]:
         for v in bad:

@@ -309,12 +309,13 @@ def test_steady_state_matches_direct_solve(quac, oracle):
     (3, 4, dict(omega=0.45, delta=-0.7, kappa=0.02, gamma=1e-3)),
     (4, 6, dict(omega=0.2, delta=0.5, kappa=0.15, gamma=2e-3))], ids=["tc32", "tc32-slow", "tc96"])
 def test_steady_state_preconditioned_vs_plain(quac, oracle, ne, nc, params):
-    """The no-jump-inverse preconditioner: the same residual and populations
-    against a direct solve, in at least ten times fewer iterations than the
-    unpreconditioned GMRES(100)."""
+    """The no-jump-inverse preconditioner, exact (1) and from the Hermitian
+    part of H_eff (2): the same residual and populations against a direct
+    solve, in at least ten times fewer iterations than the unpreconditioned
+    GMRES(100)."""
     import scipy.sparse.linalg as sla
     its, xs = {}, {}
-    for pre in (0, 1):
+    for pre in (0, 1, 2):
         S = H.ProductSystem(quac)
         H.tavis_cummings(S, ne=ne, nc=nc, **params)
         quac.construct_matrix(S.qs)
@@ -323,7 +324,7 @@ def test_steady_state_preconditioned_vs_plain(quac, oracle, ne, nc, params):
         try:
             its[pre] = quac.steady_state_sys(S.qs, x)
         finally:
-            quac.set_gmres_preconditioner(1)
+            quac.set_gmres_preconditioner(2)
         xs[pre] = x.to_numpy()
         x.destroy()
         S.qs.destroy()
@@ -338,17 +339,18 @@ def test_steady_state_preconditioned_vs_plain(quac, oracle, ne, nc, params):
     b[0] = 1
     xd = sla.spsolve(A.tocsc(), b)
     pops = lambda v: np.real(np.diag(v.reshape(D, D, order="F")))
-    for pre in (0, 1):
+    for pre in (0, 1, 2):
         assert its[pre] > 0
         assert np.linalg.norm(A @ xs[pre] - b) < 1e-10
         assert np.max(np.abs(pops(xs[pre]) - pops(xd))) < 1e-8
     assert 10 * its[1] <= its[0], its
+    assert 10 * its[2] <= its[0], its
 
 
 def test_legacy_steady_state_uses_preconditioner(quac):
     """steady_state(Vec) and steady_state_sys share the solver; the option is
-    process-wide and defaults to on."""
-    assert quac.lib().quac_set_gmres_preconditioner(1) == 0
+    process-wide and defaults to on (the Hermitian-part form)."""
+    assert quac.lib().quac_set_gmres_preconditioner(2) == 0
 
 
 def test_monitor_called_every_step(quac):

@@ -69,7 +69,7 @@ def no_precond(quac):
     """The unpreconditioned solver (the deflation flow's setting)."""
     quac.set_gmres_preconditioner(0)
     yield
-    quac.set_gmres_preconditioner(1)
+    quac.set_gmres_preconditioner(2)
 
 
 def _factors(x, D, r):
@@ -279,7 +279,7 @@ def test_trained_network_proposals_and_measured_gain(quac):
     try:
         _run_deflation_flow(quac, WS, net, untrained, train, held, ne, nc, D)
     finally:
-        quac.set_gmres_preconditioner(1)
+        quac.set_gmres_preconditioner(2)
         net.destroy()
         untrained.destroy()
 

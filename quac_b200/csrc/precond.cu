@@ -40,8 +40,11 @@ struct Decomp {
   int device = 0;
   double shift = 0.0;
   double2 *V = nullptr, *Vi = nullptr, *lam = nullptr;
+  float2 *V32 = nullptr, *Vi32 = nullptr;  // complex64 copies for the complex64-basis GMRES
   ~Decomp() {
     for (double2 *p : {V, Vi, lam})
+      if (p) cudaFree(p);
+    for (float2 *p : {V32, Vi32})
       if (p) cudaFree(p);
   }
 };
@@ -52,7 +55,8 @@ struct DeviceCtx {
   cusolverDnParams_t par = nullptr;
   cublasHandle_t blas = nullptr;
   double2 *T = nullptr, *Z = nullptr;
-  size_t cap = 0;  // elements of T and Z
+  float2 *T32 = nullptr, *U32 = nullptr;
+  size_t cap = 0;  // elements of T and Z (and of T32, U32)
 };
 
 struct SteadyPrecond {
@@ -98,6 +102,44 @@ __global__ void k_herm_eigs(const double2 *__restrict__ U, const double2 *__rest
   if (threadIdx.x == 0) lam[k] = make_double2(w[k], -0.5 * red[0]);
 }
 
+__global__ void k_to_c64(const double2 *__restrict__ x, float2 *__restrict__ y, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * PT + threadIdx.x; i < n; i += (int64_t)gridDim.x * PT)
+    y[i] = make_float2((float)x[i].x, (float)x[i].y);
+}
+
+__global__ void k_to_c128(const float2 *__restrict__ x, double2 *__restrict__ y, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * PT + threadIdx.x; i < n; i += (int64_t)gridDim.x * PT)
+    y[i] = make_double2((double)x[i].x, (double)x[i].y);
+}
+
+// complex64 form of k_sylvester_scale (divisor in double)
+__global__ void k_sylvester_scale32(float2 *__restrict__ y, const double2 *__restrict__ lam, int D, double shift) {
+  const int64_t n = (int64_t)D * D;
+  for (int64_t i = (int64_t)blockIdx.x * PT + threadIdx.x; i < n; i += (int64_t)gridDim.x * PT) {
+    const int k = (int)(i / D), j = (int)(i - (int64_t)k * D);
+    const double2 a = lam[j], b = lam[k];
+    const double dr = a.y + b.y - shift, di = b.x - a.x;
+    const double inv = 1.0 / (dr * dr + di * di);
+    const float2 v = y[i];
+    y[i] = make_float2((float)((v.x * dr + v.y * di) * inv), (float)((v.y * dr - v.x * di) * inv));
+  }
+}
+
+int grid_of(int64_t n) { return (int)std::min<int64_t>((n + PT - 1) / PT, 148 * 8); }
+
+// complex64 copies of V and V^-1
+bool add_c64_copies(Decomp &P, cudaStream_t s) {
+  const int64_t n2 = (int64_t)P.D * P.D;
+  QCUDA(cudaMalloc(&P.V32, n2 * sizeof(float2)));
+  QCUDA(cudaMalloc(&P.Vi32, n2 * sizeof(float2)));
+  if (has_error()) return false;
+  k_to_c64<<<grid_of(n2), PT, 0, s>>>(P.V, P.V32, n2);
+  k_to_c64<<<grid_of(n2), PT, 0, s>>>(P.Vi, P.Vi32, n2);
+  count_launch(2);
+  QCUDA(cudaStreamSynchronize(s));
+  return !has_error();
+}
+
 bool blas_ok(cublasStatus_t st, const char *what) {
   if (st == CUBLAS_STATUS_SUCCESS) return true;
   fail(9, "ERROR! %s failed (cuBLAS status %d)\n", what, (int)st);
@@ -130,12 +172,17 @@ DeviceCtx *device_ctx() {
 
 bool ensure_scratch(DeviceCtx &C, size_t n2) {
   if (C.cap >= n2) return true;
-  if (C.T) cudaFree(C.T);
-  if (C.Z) cudaFree(C.Z);
+  for (double2 *p : {C.T, C.Z})
+    if (p) cudaFree(p);
+  for (float2 *p : {C.T32, C.U32})
+    if (p) cudaFree(p);
   C.T = C.Z = nullptr;
+  C.T32 = C.U32 = nullptr;
   C.cap = 0;
   QCUDA(cudaMalloc(&C.T, n2 * sizeof(double2)));
   QCUDA(cudaMalloc(&C.Z, n2 * sizeof(double2)));
+  QCUDA(cudaMalloc(&C.T32, n2 * sizeof(float2)));
+  QCUDA(cudaMalloc(&C.U32, n2 * sizeof(float2)));
   if (has_error()) return false;
   C.cap = n2;
   return true;
@@ -244,7 +291,7 @@ std::shared_ptr<Decomp> decompose(qsystem qs, DeviceCtx &C, cudaStream_t s) {
   if (options().gmres_precond == 2) {
     if (!ensure_scratch(C, n2)) return nullptr;
     auto Q = decompose_hermitian(D, H, C, s);
-    if (!Q) return nullptr;
+    if (!Q || !add_c64_copies(*Q, s)) return nullptr;
     g_builds++;
     g_build_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return Q;
@@ -313,7 +360,7 @@ std::shared_ptr<Decomp> decompose(qsystem qs, DeviceCtx &C, cudaStream_t s) {
   }
   for (void *p : {(void *)A, (void *)ipiv, (void *)info, dwork})
     if (p) cudaFree(p);
-  if (!ok || has_error()) return nullptr;
+  if (!ok || has_error() || !add_c64_copies(*P, s)) return nullptr;
   g_builds++;
   g_build_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return P;
@@ -367,6 +414,30 @@ void precond_apply(SteadyPrecond &P, const double2 *x, double2 *y, cudaStream_t 
   count_launch();
   blas_ok(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one, cV, D, cy, D, &zero, cT, D), "zgemm");
   blas_ok(cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, D, D, D, &one, cT, D, cV, D, &zero, cy, D), "zgemm");
+}
+
+// y = L0^-1 x with x a complex64 vector and the four GEMMs in complex64
+// (the complex64-basis GMRES: its Arnoldi vectors are complex64 already,
+// and GMRES only needs the preconditioner to be a fixed map)
+void precond_apply_c64(SteadyPrecond &P, const float2 *x, double2 *y, cudaStream_t s) {
+  const Decomp &M = *P.dec;
+  const int D = M.D;
+  const cuComplex one = make_cuComplex(1.0f, 0.0f), zero = make_cuComplex(0.0f, 0.0f);
+  auto *cx = reinterpret_cast<const cuComplex *>(x);
+  auto *cT = reinterpret_cast<cuComplex *>(P.ctx->T32);
+  auto *cU = reinterpret_cast<cuComplex *>(P.ctx->U32);
+  auto *cV = reinterpret_cast<const cuComplex *>(M.V32);
+  auto *cVi = reinterpret_cast<const cuComplex *>(M.Vi32);
+  cublasHandle_t h = P.ctx->blas;
+  blas_ok(cublasSetStream(h, s), "cublasSetStream");
+  blas_ok(cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one, cVi, D, cx, D, &zero, cT, D), "cgemm");
+  blas_ok(cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, D, D, D, &one, cT, D, cVi, D, &zero, cU, D), "cgemm");
+  const int64_t n2 = (int64_t)D * D;
+  k_sylvester_scale32<<<grid_of(n2), PT, 0, s>>>(P.ctx->U32, M.lam, D, M.shift);
+  blas_ok(cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, D, D, D, &one, cV, D, cU, D, &zero, cT, D), "cgemm");
+  blas_ok(cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_C, D, D, D, &one, cT, D, cV, D, &zero, cU, D), "cgemm");
+  k_to_c128<<<grid_of(n2), PT, 0, s>>>(P.ctx->U32, y, n2);
+  count_launch(2);
 }
 
 double2 *precond_scratch(SteadyPrecond &P) { return P.ctx->Z; }

@@ -756,6 +756,7 @@ static Gmres &gmres_for(qsystem) { return gmres_slot().g; }
 struct SteadyPrecond;
 SteadyPrecond *precond_for(qsystem qs, cudaStream_t s);
 void precond_apply(SteadyPrecond &P, const double2 *x, double2 *y, cudaStream_t s);
+void precond_apply_c64(SteadyPrecond &P, const float2 *x, double2 *y, cudaStream_t s);
 double2 *precond_scratch(SteadyPrecond &P);
 
 // A x with A = L + e0 vec(I)^T
@@ -1256,14 +1257,17 @@ static int64_t gmres_run(const DeviceProgram &PP, Gmres &G, double2 *x, double r
       const double2 *src;
       if constexpr (std::is_same<VT, double2>::value) {
         src = reinterpret_cast<const double2 *>(vj);
+        if (pre) {  // w = A M^-1 v_j
+          precond_apply(*pre, src, precond_scratch(*pre), s);
+          src = precond_scratch(*pre);
+        }
+      } else if (pre) {  // complex64 basis: M^-1 applied in complex64
+        precond_apply_c64(*pre, reinterpret_cast<const float2 *>(vj), precond_scratch(*pre), s);
+        src = precond_scratch(*pre);
       } else {
         k_scale<<<grid_for(n), NT, 0, s>>>(vj, G.t, n, 1.0);
         count_launch();
         src = G.t;
-      }
-      if (pre) {  // w = A M^-1 v_j
-        precond_apply(*pre, src, precond_scratch(*pre), s);
-        src = precond_scratch(*pre);
       }
       apply_A(PP, src, G.w, s);
       if (def) apply_P(PP, *def, G.w, n, s);  // Arnoldi on P A

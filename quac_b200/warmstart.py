@@ -173,9 +173,9 @@ def measure_sweep(q, a):
     cold     unpreconditioned complex128 GMRES(100) from e0 (on the first
              a.cold_sample points when set), the plain path;
     method   the learned run's solver without the network: with a.precond,
-             complex128 GMRES(100) preconditioned by the point's own
-             eigen-decomposition; otherwise the guided solver with the first
-             kd unit vectors as deflation space; both from e0;
+             GMRES(100) preconditioned by the point's own decomposition, in
+             the a.fp32 basis precision; otherwise the guided solver with the
+             first kd unit vectors as deflation space; both from e0;
     learned  the network's proposal as start (the better of it and e0 by
              residual), with a.precond preconditioned GMRES(100) in the
              a.fp32 basis precision, otherwise with the proposal's deflation
@@ -202,8 +202,6 @@ def measure_sweep(q, a):
 
     def method_settings():
         learned_settings()
-        if a.precond:
-            q.set_gmres_precision(0)
 
     def plain_settings():
         q.set_gmres_preconditioner(0)
@@ -278,7 +276,7 @@ def measure_sweep(q, a):
         "solver": ("GMRES(100) preconditioned by the "
                    + ("exact inverse" if a.precond == 1 else "Hermitian-part form of the inverse")
                    + " of the no-jump Liouvillian, "
-                   + ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + " basis in the learned arm"
+                   + ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + " basis"
                    if a.precond else
                    ("fp32-inner/fp64-refined" if a.fp32 else "fp64") + f" GMRES({a.restart})"
                    + (", deflation refreshed every restart" if a.refresh else "")),

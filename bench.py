@@ -464,6 +464,7 @@ def steady_summary(q):
     return {k: out[k] for k in ("workload", "sweep", "train_states", "held_out", "rtol", "solver", "generation",
                                 "training",
                                 "cold", "method", "learned", "learned_vs_cold", "learned_vs_method",
+                                "learned_vs_method_median_point",
                                 "method_vs_cold", "decompositions", "pop_err_max", "residual_max")}
 
 
@@ -544,9 +545,12 @@ def run_ours(args, rank, world, local_rank):
     q.set_stream(qs, None)
     q.time_step_host(qs, hp, 0.0, RK_STEPS * DT, DT, 10 ** 9)
     torch.cuda.synchronize()
+    e2e_steps = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        ts = time.perf_counter()
         q.time_step_host(qs, hp, 0.0, RK_STEPS * DT, DT, 10 ** 9)
+        e2e_steps.append((time.perf_counter() - ts) * 1e3)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1e3
     from quac_b200.replicas import max_over_ranks
@@ -565,7 +569,8 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": workload_config(world),
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": 16 * n,
-                "d2h_bytes_per_step": 16 * n},
+                "d2h_bytes_per_step": 16 * n,
+                "step_ms": {"min": min(e2e_steps), "median": statistics.median(e2e_steps), "max": max(e2e_steps)}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "frac_of_nominal_8tbs": achieved / 8000.0,

@@ -282,9 +282,13 @@ def measure_sweep(q, a):
                    + (", deflation refreshed every restart" if a.refresh else "")),
         "generation": {"seconds": t_gen, "mean_iterations": float(np.mean(gen_its))},
         "training": {"steps": a.steps, "seconds": t_train, "loss": loss},
-        "method": {"solves_per_s": n / r[:, 3].sum(), "iterations": r[:, 2].astype(int).tolist()},
-        "learned": {"solves_per_s": n / r[:, 5].sum(), "iterations": r[:, 4].astype(int).tolist()},
+        "method": {"solves_per_s": n / r[:, 3].sum(), "iterations": r[:, 2].astype(int).tolist(),
+                   "seconds": [round(float(v), 4) for v in r[:, 3]]},
+        "learned": {"solves_per_s": n / r[:, 5].sum(), "iterations": r[:, 4].astype(int).tolist(),
+                    "seconds": [round(float(v), 4) for v in r[:, 5]]},
         "learned_vs_method": r[:, 3].sum() / r[:, 5].sum(),
+        # per-point time ratios are less sensitive to an occasional slow setup
+        "learned_vs_method_median_point": float(np.median(r[:, 3] / r[:, 5])),
         "pop_err_max": float(r[:, 6].max()),
         "residual_max": float(r[:, 7].max()),
     }

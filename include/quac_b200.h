@@ -486,10 +486,12 @@ int quac_set_gmres_restart(int m);
  * (half the Gram-Schmidt traffic), while L.x, the projections, the
  * iterate and the residual b - A x formed at every restart stay
  * complex128, so each restart refines the solution to the same
- * complex128 tolerance.  If the true residual has not fallen below 0.9x
- * its value 20 restarts earlier (the complex64 rounding of the basis
- * then costs more than a cycle gains, as on ill-conditioned systems),
- * the solve continues with a complex128 basis. */
+ * complex128 tolerance; the steady-state preconditioner, when on, is then
+ * applied to the complex64 vectors in complex64 as well.  If the true
+ * residual has not fallen below 0.9x its value 20 restarts earlier (the
+ * complex64 rounding of the basis then costs more than a cycle gains, as
+ * on ill-conditioned systems), the solve continues with a complex128
+ * basis. */
 int quac_set_gmres_precision(int precision);
 /* Deflation refresh of quac_steady_state_guided (no reference
  * counterpart): 1 (default) = at every restart after the first, the

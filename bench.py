@@ -614,7 +614,7 @@ def run_profile(args):
       --profile ensemble --instances N --t-end T [--fp32]          one persistent ensemble launch
       --profile gemm     --m M --n N --k K --reps R                 TF32 tensor-core GEMM
       --profile steady   --ne E --nc C --train T --held H --kd K --restart M --fp32-basis B --sweep2d
-                         --precond P --cold-sample S --train-steps N   one steady-state sweep
+                         --precond P --cold-sample S --train-steps N --rtol R   one steady-state sweep
                                                                      learned warm-start sweep
     """
     import ctypes
@@ -690,7 +690,8 @@ def run_profile(args):
         from quac_b200 import warmstart
         a = warmstart.sweep_settings(ne=args.ne, nc=args.nc, train=args.train, held=args.held, kd=args.kd,
                                      restart=args.restart, fp32=args.fp32_basis, sweep2d=args.sweep2d,
-                                     precond=args.precond, cold_sample=args.cold_sample, steps=args.train_steps)
+                                     precond=args.precond, cold_sample=args.cold_sample, steps=args.train_steps,
+                                     rtol=args.rtol)
         print(json.dumps(warmstart.measure_sweep(q, a)))
 
 
@@ -726,6 +727,7 @@ def main():
     ap.add_argument("--precond", type=int, default=1)
     ap.add_argument("--cold-sample", type=int, default=None)
     ap.add_argument("--train-steps", type=int, default=8000)
+    ap.add_argument("--rtol", type=float, default=1e-11)
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

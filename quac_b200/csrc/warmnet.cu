@@ -83,21 +83,34 @@ __global__ void k_gather_inputs(const float *__restrict__ X, const int *__restri
   Xb[i] = (b < nb) ? X[(size_t)idx[b] * IN_PAD + k] : 0.f;
 }
 
-// S_b = F_b^H F_b  (r x r) for each batch row b < nb
+// S_b = F_b^H F_b  (r x r) for each batch row b < nb; F_b staged in
+// shared memory 64 rows at a time, transposed so that a warp's threads
+// (consecutive j) read consecutive words
 __global__ void k_gram(const float *__restrict__ Fo, int D, int r, int nb, float2 *__restrict__ S) {
+  constexpr int KC = 64;
+  __shared__ float2 Fs[KC][16];
   const int b = blockIdx.x;
   if (b >= nb) return;
   const float2 *F = reinterpret_cast<const float2 *>(Fo + (size_t)b * 2 * D * r);
-  for (int q = threadIdx.x; q < r * r; q += blockDim.x) {
-    const int i = q / r, j = q % r;
-    float ax = 0.f, ay = 0.f;
-    for (int k = 0; k < D; k++) {
-      const float2 u = F[(size_t)i * D + k], w = F[(size_t)j * D + k];
-      ax += u.x * w.x + u.y * w.y;  // conj(u) w
-      ay += u.x * w.y - u.y * w.x;
+  const int q = threadIdx.x, i = q / r, j = q % r;
+  const bool mine = q < r * r;
+  float ax = 0.f, ay = 0.f;
+  for (int k0 = 0; k0 < D; k0 += KC) {
+    const int kn = min(KC, D - k0);
+    for (int e = threadIdx.x; e < KC * r; e += blockDim.x) {
+      const int jj = e / KC, kk = e % KC;
+      Fs[kk][jj] = kk < kn ? F[(size_t)jj * D + k0 + kk] : make_float2(0.f, 0.f);
     }
-    S[(size_t)b * r * r + q] = make_float2(ax, ay);
+    __syncthreads();
+    if (mine)
+      for (int kk = 0; kk < kn; kk++) {
+        const float2 u = Fs[kk][i], w = Fs[kk][j];
+        ax += u.x * w.x + u.y * w.y;  // conj(u) w
+        ay += u.x * w.y - u.y * w.x;
+      }
+    __syncthreads();
   }
+  if (mine) S[(size_t)b * r * r + q] = make_float2(ax, ay);
 }
 
 // G_b = rho_{idx[b]} F_b  (D x r), rho column-major complex64; one thread per row
@@ -118,7 +131,25 @@ __global__ void k_rho_f(const float *__restrict__ Fo, const float2 *__restrict__
   float ax[16], ay[16];
 #pragma unroll
   for (int j = 0; j < 16; j++) { ax[j] = 0.f; ay[j] = 0.f; }
-  for (int c = 0; c < D; c++) {
+  // eight loads of the column walk in flight before their products
+  int c = 0;
+  for (; c + 8 <= D; c += 8) {
+    float2 xb[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) xb[u] = R[(size_t)(c + u) * D + row];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        if (j < r) {
+          const float2 f = Fs[(c + u) * r + j];
+          ax[j] += xb[u].x * f.x - xb[u].y * f.y;
+          ay[j] += xb[u].x * f.y + xb[u].y * f.x;
+        }
+      }
+    }
+  }
+  for (; c < D; c++) {
     const float2 x = R[(size_t)c * D + row];
 #pragma unroll
     for (int j = 0; j < 16; j++) {

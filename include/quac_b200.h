@@ -295,6 +295,13 @@ PetscInt steady_state_sys(qsystem qsys, qvec x);
 int quac_lrho_apply_device(qsystem qsys, const void *x_dev, void *y_dev);
 /* Same on host buffers: copies x in, applies L, copies y out. */
 int quac_lrho_apply_host(qsystem qsys, const PetscScalar *x_host, PetscScalar *y_host);
+/* No counterpart in the reference (a QuaC program would MatView its mat_A,
+ * qsystem.c:957-963, onto a binary viewer): writes the operator the
+ * system's terms define -- the D^2 x D^2 Liouvillian in the column-stacked
+ * ordering, or -i H for a wavefunction system -- as a PETSc binary AIJ
+ * matrix with 64-bit indices (the format MatLoad reads and the reference's
+ * test fixtures use), built on the host from the compiled term tables. */
+int quac_write_superoperator_binary(qsystem qsys, const char *filename);
 /* No reference counterpart.  quac_lrho_apply_device without any device
  * allocation at call time, for callers that must not allocate inside their
  * loop: a framework whose memory pool already holds the device's memory, or

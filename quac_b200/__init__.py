@@ -156,6 +156,7 @@ def lib():
         "steady_state_sys": (i64, [P(_QsysStruct), P(_QvecStruct)]),
         "quac_lrho_apply_device": (ctypes.c_int, [P(_QsysStruct), vp, vp]),
         "quac_lrho_apply_host": (ctypes.c_int, [P(_QsysStruct), vp, vp]),
+        "quac_write_superoperator_binary": (ctypes.c_int, [P(_QsysStruct), ctypes.c_char_p]),
         "quac_time_step_host": (ctypes.c_int, [P(_QsysStruct), vp, dbl, dbl, dbl, i64]),
         "quac_set_error_mode": (None, [ctypes.c_int]),
         "quac_last_error": (ctypes.c_char_p, []),
@@ -753,6 +754,30 @@ def lrho_apply_device(qs, x_ptr, y_ptr):
     """y = L x on device buffers (qs.dim complex128 each)."""
     lib().quac_lrho_apply_device(qs._ptr, vp(x_ptr), vp(y_ptr))
     _check()
+
+
+def write_superoperator_binary(qs, filename):
+    """Writes the system's operator (Liouvillian, or -i H for a wavefunction
+    system) as a PETSc binary AIJ matrix (64-bit indices, big endian)."""
+    lib().quac_write_superoperator_binary(qs._ptr, os.fsencode(filename))
+    _check()
+
+
+def read_petsc_binary_matrix(filename):
+    """(shape, rowptr, cols, values) of a PETSc binary AIJ matrix written
+    with 64-bit indices and complex128 values."""
+    raw = open(filename, "rb").read()
+    head = np.frombuffer(raw[:32], dtype=">i8")
+    if head[0] != 1211216:
+        raise ValueError(f"{filename}: not a PETSc binary matrix (class id {head[0]})")
+    m, n, nz = (int(v) for v in head[1:])
+    off = 32
+    lens = np.frombuffer(raw[off:off + 8 * m], dtype=">i8").astype(np.int64)
+    off += 8 * m
+    cols = np.frombuffer(raw[off:off + 8 * nz], dtype=">i8").astype(np.int64)
+    off += 8 * nz
+    vals = np.frombuffer(raw[off:off + 16 * nz], dtype=">c16").astype(np.complex128)
+    return (m, n), np.concatenate([[0], np.cumsum(lens)]), cols, vals
 
 
 def lrho_apply_host(qs, x):

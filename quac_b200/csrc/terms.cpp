@@ -368,3 +368,93 @@ extern "C" int quac_program_export(qsystem qs, int mode, int64_t *counts, int *m
     for (auto &z : *v) { vals[vi++] = z.real(); vals[vi++] = z.imag(); }
   return 0;
 }
+
+namespace {
+
+// Entries (column, value) of row i of the compiled operator, merged by
+// column in ascending order; the diagonal is always present.  Density
+// matrices: i = c D + r (column stacking); wavefunctions: i = r.
+void operator_row(const quac::HostProg &hp, int64_t i, std::vector<std::pair<int64_t, quac::cplx>> &row) {
+  using quac::cplx;
+  const int64_t D = hp.D;
+  row.clear();
+  if (hp.ncols == 1) {
+    const int r = (int)i;
+    row.emplace_back(i, hp.dr[r]);
+    for (size_t t = 0; t < hp.Lmap.size(); t++)
+      if (hp.Lmap[t][r] >= 0) row.emplace_back(hp.Lmap[t][r], hp.Lval[t][r]);
+  } else {
+    const int c = (int)(i / D), r = (int)(i - (int64_t)c * D);
+    cplx d = hp.dr[r] + hp.dc[c];
+    for (size_t t = 0; t < hp.Jdrow.size(); t++) d += hp.Jdrow[t][r] * hp.Jdcol[t][c];
+    row.emplace_back(i, d);
+    for (size_t t = 0; t < hp.Lmap.size(); t++)
+      if (hp.Lmap[t][r] >= 0) row.emplace_back((int64_t)c * D + hp.Lmap[t][r], hp.Lval[t][r]);
+    for (size_t t = 0; t < hp.Rmap.size(); t++)
+      if (hp.Rmap[t][c] >= 0) row.emplace_back((int64_t)hp.Rmap[t][c] * D + r, hp.Rval[t][c]);
+    for (size_t t = 0; t < hp.Jmap.size(); t++)
+      if (hp.Jmap[t][r] >= 0 && hp.Jmap[t][c] >= 0)
+        row.emplace_back((int64_t)hp.Jmap[t][c] * D + hp.Jmap[t][r], hp.Jrow[t][r] * hp.Jcol[t][c]);
+  }
+  std::sort(row.begin(), row.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+  size_t k = 0;
+  for (size_t j = 0; j < row.size(); j++) {
+    if (k > 0 && row[k - 1].first == row[j].first) row[k - 1].second += row[j].second;
+    else row[k++] = row[j];
+  }
+  row.resize(k);
+}
+
+bool put_be64(FILE *f, uint64_t v) {
+  v = __builtin_bswap64(v);
+  return fwrite(&v, 8, 1, f) == 1;
+}
+
+bool put_be_double(FILE *f, double x) {
+  uint64_t v;
+  std::memcpy(&v, &x, 8);
+  return put_be64(f, v);
+}
+
+}  // namespace
+
+// No counterpart in the reference, which only prints a summary of mat_A
+// (solver.c:120-124); a QuaC user reaches the assembled operator with
+// MatView on a binary viewer.  Here the operator is never assembled, so
+// this writes it from the compiled term tables in PETSc's binary AIJ
+// format with 64-bit indices (big endian: class id 1211216, M, N, nz, row
+// lengths, column indices, complex128 values), the format of the
+// reference's own test fixtures, without touching the GPU.  Density
+// matrices give the D^2 x D^2 Liouvillian in the column-stacked ordering,
+// wavefunctions the D x D Schroedinger operator -i H.
+extern "C" int quac_write_superoperator_binary(qsystem qs, const char *filename) {
+  using namespace quac;
+  if (!filename) { fail(0, "ERROR! quac_write_superoperator_binary: no file name\n"); return 1; }
+  HostProg hp;
+  const int mode = qs->dm_equations ? 0 : 1;
+  if (!compile_host(qs, mode, hp)) return 1;
+  const int64_t n = hp.ncols == 1 ? (int64_t)hp.D : (int64_t)hp.D * hp.D;
+  FILE *f = fopen(filename, "wb");
+  if (!f) { fail(0, "ERROR! quac_write_superoperator_binary: cannot open %s\n", filename); return 1; }
+  std::vector<std::pair<int64_t, cplx>> row;
+  std::vector<int64_t> lens(n);
+  int64_t nz = 0;
+  for (int64_t i = 0; i < n; i++) {
+    operator_row(hp, i, row);
+    lens[i] = (int64_t)row.size();
+    nz += lens[i];
+  }
+  bool ok = put_be64(f, 1211216) && put_be64(f, n) && put_be64(f, n) && put_be64(f, nz);
+  for (int64_t i = 0; ok && i < n; i++) ok = put_be64(f, lens[i]);
+  for (int64_t i = 0; ok && i < n; i++) {
+    operator_row(hp, i, row);
+    for (auto &e : row) ok = ok && put_be64(f, (uint64_t)e.first);
+  }
+  for (int64_t i = 0; ok && i < n; i++) {
+    operator_row(hp, i, row);
+    for (auto &e : row) ok = ok && put_be_double(f, e.second.real()) && put_be_double(f, e.second.imag());
+  }
+  if (fclose(f) != 0) ok = false;
+  if (!ok) { fail(0, "ERROR! quac_write_superoperator_binary: writing %s failed\n", filename); return 1; }
+  return 0;
+}

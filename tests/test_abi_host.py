@@ -122,6 +122,27 @@ def test_term_compiler_reproduces_fixture(quac, golden, case):
     B.qs.destroy()
 
 
+@pytest.mark.parametrize("case", F.CASES, ids=lambda c: f"{c[0]}-{c[1]}op-{c[2]}-{'c' if c[3] else 'r'}")
+def test_superoperator_binary_matches_fixture(quac, golden, case, tmp_path):
+    """The operator written in PETSc's binary AIJ format (the format of the
+    reference's fixtures) reads back as the fixture matrix; rows are sorted
+    by column with the diagonal always present."""
+    fam, nop, kind, cplx = case
+    B = _Builder(quac)
+    stems = F.build(B, fam, nop, kind, cplx)
+    path = tmp_path / "op.dat"
+    quac.write_superoperator_binary(B.qs, str(path))
+    (m, n), rowptr, cols, vals = quac.read_petsc_binary_matrix(str(path))
+    A = sp.csr_matrix((vals, cols, rowptr), shape=(m, n))
+    ref = sum(golden_csr(golden, s) for s in stems)
+    assert (m, n) == ref.shape
+    assert sp.linalg.norm(A - ref) <= 1e-9
+    for i in range(m):
+        row = cols[rowptr[i]:rowptr[i + 1]]
+        assert np.all(np.diff(row) > 0) and i in row
+    B.qs.destroy()
+
+
 def test_term_compiler_vec_ops_match_oracle(quac, oracle):
     q = quac
     qs = q.initialize_system()

@@ -261,6 +261,8 @@ void add_lin(PetscScalar a, op_handle op);              /* operators.c:679-719 *
 void add_lin_mult2(PetscScalar a, op_handle op1, op_handle op2);      /* operators.c:743-821 */
 void steady_state(Vec x);                               /* solver.c:33-221 */
 void set_ts_monitor(quac_ts_monitor monitor);           /* solver.c:526-532 */
+void set_ts_monitor_ctx(quac_ts_monitor monitor, void *ctx);            /* solver.c:542-545 */
+void time_step(Vec x, PetscReal init_time, PetscReal time_max, PetscReal dt, PetscInt steps_max); /* solver.c:236-510 */
 void create_full_dm(Vec *dm);                           /* dm_utilities.c:635-655 */
 void create_dm(Vec *dm, PetscInt size);                 /* dm_utilities.c:616-623 */
 void destroy_dm(Vec dm);                                /* dm_utilities.c:1029-1032 */

@@ -217,6 +217,9 @@ def lib():
         "add_lin": (None, [Scalar, _OpPtr]),
         "add_lin_mult2": (None, [Scalar, _OpPtr, _OpPtr]),
         "steady_state": (None, [vp]),
+        "time_step": (None, [vp, dbl, dbl, dbl, i64]),
+        "set_ts_monitor_ctx": (None, [vp, vp]),
+        "QuaC_clear": (None, []),
         "create_full_dm": (None, [P(vp)]),
         "create_dm": (None, [P(vp), i64]),
         "destroy_dm": (None, [vp]),
@@ -1131,6 +1134,38 @@ def get_dm_element(dm, row, col):
 def steady_state(dm):
     """solver.c:33-221 on the legacy system, result in dm."""
     lib().steady_state(dm._ptr)
+    _check()
+
+
+_legacy_monitor = None
+
+
+def set_ts_monitor(fn):
+    """fn(step, time, vec_handle) after each step of the legacy time_step
+    (solver.c:526-545); None clears."""
+    global _legacy_monitor
+    if fn is None:
+        _legacy_monitor = None
+        lib().set_ts_monitor_ctx(None, None)
+        return
+
+    def _cb(ts, step, t, vec, ctx):
+        fn(step, t, vec)
+        return 0
+
+    _legacy_monitor = _MonitorFn(_cb)
+    lib().set_ts_monitor_ctx(ctypes.cast(_legacy_monitor, vp), None)
+
+
+def time_step(dm, t0, tmax, dt, steps_max):
+    """solver.c:236-510: the legacy system integrated on dm (a LegacyVec)."""
+    lib().time_step(dm._ptr, float(t0), float(tmax), float(dt), int(steps_max))
+    _check()
+
+
+def QuaC_clear():
+    """quac.c:60-80: forget the legacy global system so a new one can be built."""
+    lib().QuaC_clear()
     _check()
 
 

@@ -209,7 +209,11 @@ void QuaC_initialize(int argc, char **args) {
 }
 
 void QuaC_finalize(void) { g_initialized = false; }
-void QuaC_clear(void) {}
+static void legacy_clear();
+// quac.c:60-80: forgets the legacy global system (its terms and operator
+// matrix) so that a program can build a new one; the operators created
+// with create_op stay the caller's to destroy, as in the reference
+void QuaC_clear(void) { legacy_clear(); }
 
 int PetscPrintf(int comm, const char *fmt, ...) {
   (void)comm;
@@ -1217,7 +1221,41 @@ void add_lin(PetscScalar a, op_handle op) { add_lin_term(legacy(), a, 1, op); }
 void add_lin_mult2(PetscScalar a, op_handle o1, op_handle o2) { add_lin_term(legacy(), a, 2, o1, o2); }
 
 static quac_ts_monitor g_legacy_monitor = nullptr;
-void set_ts_monitor(quac_ts_monitor monitor) { g_legacy_monitor = monitor; }
+static void *g_legacy_ctx = nullptr;
+void set_ts_monitor(quac_ts_monitor monitor) {
+  g_legacy_monitor = monitor;
+  g_legacy_ctx = nullptr;
+}
+void set_ts_monitor_ctx(quac_ts_monitor monitor, void *ctx) {
+  g_legacy_monitor = monitor;
+  g_legacy_ctx = ctx;
+}
+
+static void legacy_clear() {
+  if (g_legacy) destroy_system(&g_legacy);
+  g_legacy = nullptr;
+  g_legacy_monitor = nullptr;
+  g_legacy_ctx = nullptr;
+}
+
+// solver.c:236-510: the legacy global system integrated from init_time to
+// time_max on the caller's Vec (density matrix or wavefunction, as the
+// legacy terms define), with the monitor of set_ts_monitor(_ctx).  The
+// reference runs PETSc TS with TSRK3BS here; this runs the same
+// integrator as time_step_sys (its controller settings and -ts_* options,
+// last step matched to time_max).
+void time_step(Vec x, PetscReal init_time, PetscReal time_max, PetscReal dt, PetscInt steps_max) {
+  qsystem qs = legacy();
+  if (!qs->mat_allocated) construct_matrix(qs);
+  if (has_error()) return;
+  set_ts_monitor_sys(qs, g_legacy_monitor, g_legacy_ctx);
+  qvec tmp = (qvec)calloc(1, sizeof(*tmp));
+  tmp->my_type = qs->dm_equations ? DENSITY_MATRIX : WAVEFUNCTION;
+  tmp->n = x->n;
+  tmp->data = x;
+  time_step_sys(qs, tmp, init_time, time_max, dt, steps_max);
+  free(tmp);
+}
 
 void steady_state(Vec x) {
   qsystem qs = legacy();

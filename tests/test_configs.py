@@ -256,6 +256,53 @@ def test_legacy_steady_state_matches_direct_solve(quac, oracle):
     rho.destroy()
 
 
+def test_legacy_time_step_matches_time_step_sys(quac):
+    """time_step(Vec) on the legacy global system (solver.c:236-510) after
+    QuaC_clear (quac.c:60-80) gives the state time_step_sys gives for the
+    same terms, and calls the set_ts_monitor callback at every step."""
+    q = quac
+    q.QuaC_clear()
+    qb = q.create_op(2)
+    cav = q.create_op(5)
+    q.add_to_ham(0.2, cav.n)
+    q.add_to_ham_mult2(0.1, cav.dag, qb)
+    q.add_to_ham_mult2(0.1, cav, qb.dag)
+    q.add_to_ham(0.15, cav)
+    q.add_to_ham(0.15, cav.dag)
+    q.add_lin(0.05, cav)
+    q.add_lin(2e-3, qb)
+    rho = q.create_full_dm()
+    q.add_value_to_dm(rho, 5, 5, 1.0)  # emitter excited, cavity empty
+    q.assemble_dm(rho)
+    steps = []
+    q.set_ts_monitor(lambda step, t, vec: steps.append((step, t)))
+    try:
+        q.time_step(rho, 0.0, 2.0, 0.05, 10 ** 6)
+    finally:
+        q.set_ts_monitor(None)
+    x = rho.to_numpy()
+    rho.destroy()
+    q.QuaC_clear()
+    S = H.ProductSystem(q)
+    sq, sc = S.op(2), S.op(5)
+    S.ham(0.2, sc.n)
+    S.ham(0.1, sc.dag, sq.a)
+    S.ham(0.1, sc.a, sq.dag)
+    S.ham(0.15, sc.a)
+    S.ham(0.15, sc.dag)
+    S.lin(0.05, sc.a)
+    S.lin(2e-3, sq.a)
+    q.construct_matrix(S.qs)
+    r2 = q.create_qvec_sys(S.qs)
+    q.add_to_qvec(r2, 1.0, 5, 5)
+    q.assemble_qvec(r2)
+    q.time_step_sys(S.qs, r2, 0.0, 2.0, 0.05, 10 ** 6)
+    assert _rel(x, r2.to_numpy()) < 1e-12
+    assert len(steps) > 1 and steps[-1][1] == pytest.approx(2.0)
+    r2.destroy()
+    S.qs.destroy()
+
+
 def test_read_reference_dm_binary_and_elements(quac, golden, tmp_path):
     """read_qvec_dm_binary on the reference's own rand_dm.dat bytes and the
     element read-back of qvec_utilities_tests.c:788-870 (column stacking:

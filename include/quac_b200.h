@@ -211,6 +211,15 @@ void create_arb_qvec(qvec *q, PetscInt nstates, qvec_type type);      /* qvec_ut
 void destroy_qvec(qvec *q);                             /* qvec_utilities.c:1076-1091 */
 void add_to_qvec(qvec q, PetscScalar alpha, ...);       /* qvec_utilities.c:919-969 */
 void add_to_qvec_loc(qvec q, PetscScalar alpha, PetscInt loc);        /* qvec_utilities.c:879-897 */
+/* Basis states by Fock occupations: (op, PetscInt fock state) pairs; the
+ * index is sum fock_i * n_before_i as in the reference (qvec_utilities.c:
+ * 996-1033), the diagonal element for a density matrix. */
+void add_to_qvec_fock_op(PetscScalar alpha, qvec q, PetscInt num_ops, ...);                 /* qvec_utilities.c:832-857 */
+void add_to_qvec_fock_op_list(PetscScalar alpha, qvec q, PetscInt num_ops, op_handle *ops,
+                              PetscInt *fock_states);                                         /* qvec_utilities.c:863-872 */
+void get_qvec_loc_fock_op(qvec q, PetscInt *loc, PetscInt num_ops, ...);                    /* qvec_utilities.c:973-994 */
+void get_qvec_loc_fock_op_list(qvec q, PetscInt *loc, PetscInt num_ops, op_handle *ops,
+                               PetscInt *fock_states);                                        /* qvec_utilities.c:996-1033 */
 void assemble_qvec(qvec q);                             /* qvec_utilities.c:1047-1066 */
 void set_qvec_from_init_excited_op(qsystem qsys, qvec q);             /* qvec_utilities.c:2540-2566 */
 void get_dm_element_qvec(qvec q, PetscInt row, PetscInt col, PetscScalar *val); /* qvec_utilities.c:322-337 */

@@ -137,6 +137,8 @@ def lib():
         "create_arb_qvec": (None, [P(P(_QvecStruct)), i64, ctypes.c_int]),
         "destroy_qvec": (None, [P(P(_QvecStruct))]),
         "add_to_qvec_loc": (None, [P(_QvecStruct), Scalar, i64]),
+        "add_to_qvec_fock_op_list": (None, [Scalar, P(_QvecStruct), i64, P(_OpPtr), vp]),
+        "get_qvec_loc_fock_op_list": (None, [P(_QvecStruct), P(i64), i64, P(_OpPtr), vp]),
         "assemble_qvec": (None, [P(_QvecStruct)]),
         "get_dm_element_qvec": (None, [P(_QvecStruct), i64, i64, P(Scalar)]),
         "get_wf_element_qvec": (None, [P(_QvecStruct), i64, P(Scalar)]),
@@ -579,6 +581,33 @@ def add_to_qvec(q, alpha, *locs):
         add_to_qvec_loc(q, alpha, D * int(locs[0]) + int(locs[1]))
     else:
         add_to_qvec_loc(q, alpha, int(locs[0]))
+
+
+def _fock_pairs(pairs):
+    if len(pairs) % 2:
+        raise QuacError("expected (op, fock state) pairs")
+    ops = pairs[0::2]
+    fock = np.ascontiguousarray([int(f) for f in pairs[1::2]], dtype=np.int64)
+    return len(ops), _oplist(ops), fock
+
+
+def get_qvec_loc_fock_op(q, *pairs):
+    """Index of the basis state with each given op in the given Fock state
+    (qvec_utilities.c:996-1033), the diagonal element for a density matrix:
+    get_qvec_loc_fock_op(q, op1, 1, op2, 0)."""
+    n, ops, fock = _fock_pairs(pairs)
+    loc = i64()
+    lib().get_qvec_loc_fock_op_list(q._ptr, ctypes.byref(loc), n, ops, fock.ctypes.data)
+    _check()
+    return loc.value
+
+
+def add_to_qvec_fock_op(alpha, q, *pairs):
+    """add_to_qvec_fock_op(alpha, q, op1, f1, op2, f2, ...)
+    (qvec_utilities.c:832-857)."""
+    n, ops, fock = _fock_pairs(pairs)
+    lib().add_to_qvec_fock_op_list(_sc(alpha), q._ptr, n, ops, fock.ctypes.data)
+    _check()
 
 
 def assemble_qvec(q):

@@ -636,6 +636,7 @@ void destroy_qvec(qvec *q) {
 
 void add_to_qvec_loc(qvec q, PetscScalar alpha, PetscInt loc) {
   if (loc > q->n || loc < 0) { fail(0, "ERROR! Adding to a qvec location that is out of range!\n"); return; }
+  if (loc == q->n) return;  // passes the reference's range check but no rank owns it: nothing is added
   Vec v = q->data;
   if (!v->host_pending) { vec_pull_host(v); v->host_pending = true; }
   v->h[loc] += cplx(alpha.real(), alpha.imag());
@@ -651,6 +652,62 @@ void add_to_qvec(qvec q, PetscScalar alpha, ...) {
   }
   va_end(ap);
   add_to_qvec_loc(q, alpha, loc);
+}
+
+// qvec_utilities.c:996-1033: the vector index of the basis state with op
+// i in Fock state fock_states[i] and every other subsystem in 0, as the
+// reference computes it: sum_i fock_i * n_before_i (its strides are the
+// levels BEFORE each subsystem, which is the position of that digit only
+// when subsystem 0 is the least significant, a quirk kept for parity), and
+// the diagonal element (loc, loc) of a density matrix.
+void get_qvec_loc_fock_op_list(qvec q, PetscInt *loc, PetscInt num_ops, op_handle *ops, PetscInt *fock_states) {
+  *loc = 0;
+  for (PetscInt i = 0; i < num_ops; i++) {
+    if (fock_states[i] >= ops[i]->my_levels || fock_states[i] < 0) {
+      fail(0, "ERROR! The Fock State must be less than the number of levels and greater than 0!\n");
+      return;
+    }
+    *loc += fock_states[i] * ops[i]->n_before;
+  }
+  if (q->my_type == DENSITY_MATRIX) {
+    *loc = (PetscInt)std::llround(std::sqrt((double)q->n)) * *loc + *loc;
+  } else if (q->my_type != WAVEFUNCTION && q->my_type != WF_ENSEMBLE) {
+    fail(0, "ERROR! qvec type not understood.");
+  }
+}
+
+// qvec_utilities.c:973-994: (op, fock state) pairs as variadic arguments
+void get_qvec_loc_fock_op(qvec q, PetscInt *loc, PetscInt num_ops, ...) {
+  std::vector<op_handle> ops(num_ops > 0 ? num_ops : 0);
+  std::vector<PetscInt> fock(ops.size());
+  va_list ap;
+  va_start(ap, num_ops);
+  for (size_t i = 0; i < ops.size(); i++) {
+    ops[i] = va_arg(ap, op_handle);
+    fock[i] = va_arg(ap, PetscInt);
+  }
+  va_end(ap);
+  get_qvec_loc_fock_op_list(q, loc, num_ops, ops.data(), fock.data());
+}
+
+// qvec_utilities.c:832-872: alpha added at that basis state
+void add_to_qvec_fock_op_list(PetscScalar alpha, qvec q, PetscInt num_ops, op_handle *ops, PetscInt *fock_states) {
+  PetscInt loc = 0;
+  get_qvec_loc_fock_op_list(q, &loc, num_ops, ops, fock_states);
+  if (!has_error()) add_to_qvec_loc(q, alpha, loc);
+}
+
+void add_to_qvec_fock_op(PetscScalar alpha, qvec q, PetscInt num_ops, ...) {
+  std::vector<op_handle> ops(num_ops > 0 ? num_ops : 0);
+  std::vector<PetscInt> fock(ops.size());
+  va_list ap;
+  va_start(ap, num_ops);
+  for (size_t i = 0; i < ops.size(); i++) {
+    ops[i] = va_arg(ap, op_handle);
+    fock[i] = va_arg(ap, PetscInt);
+  }
+  va_end(ap);
+  add_to_qvec_fock_op_list(alpha, q, num_ops, ops.data(), fock.data());
 }
 
 void assemble_qvec(qvec q) { vec_sync_to_device(q->data); }

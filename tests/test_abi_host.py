@@ -204,3 +204,29 @@ def test_solver_option_setters_validate_on_the_host(quac):
                 setter(v)
         for v in good:
             setter(v)
+
+
+def test_qvec_loc_fock_op_host(quac):
+    """qvec_utilities.c:996-1033: the index is sum_i fock_i * n_before_i, the
+    diagonal (loc, loc) for a density matrix; a Fock state outside
+    [0, levels) is an error.  Pure host arithmetic on the qvec header."""
+    import ctypes
+    import types
+    q = quac
+    qs = q.initialize_system()
+    a, b, c = q.create_op_sys(qs, 2), q.create_op_sys(qs, 3), q.create_op_sys(qs, 4)
+    assert (a.n_before, b.n_before, c.n_before) == (1, 2, 6)
+
+    def header(kind, n):
+        s = q._QvecStruct()
+        s.my_type, s.n = kind, n
+        return types.SimpleNamespace(_ptr=ctypes.pointer(s), keep=s)
+
+    wf, dm = header(q.WAVEFUNCTION, 24), header(q.DENSITY_MATRIX, 24 * 24)
+    assert q.get_qvec_loc_fock_op(wf, a, 1, b, 2, c, 3) == 1 + 2 * 2 + 3 * 6
+    assert q.get_qvec_loc_fock_op(wf, b, 1) == 2
+    assert q.get_qvec_loc_fock_op(dm, a, 1, c, 1) == 7 * 24 + 7
+    for bad in (2, -1):
+        with pytest.raises(q.QuacError):
+            q.get_qvec_loc_fock_op(wf, a, bad)
+    qs.destroy()

@@ -355,6 +355,27 @@ def test_set_qvec_from_init_excited_op(quac):
     qs.destroy()
 
 
+@pytest.mark.parametrize("kind", ["wf", "dm"])
+def test_add_to_qvec_fock_op_expectations(quac, kind):
+    """tests/qvec_utilities_tests.c test_get_expectation_value_wf_real /
+    _dm_real: |11> set through add_to_qvec_fock_op on two qubits gives
+    <n1> = <n2> = 1 and <qd1^dag qd2> = <qd2^dag qd1> = 0."""
+    q = quac
+    qs = q.initialize_system()
+    qd1, qd2 = q.create_op_sys(qs, 2), q.create_op_sys(qs, 2)
+    v = q.create_wf_sys(qs) if kind == "wf" else q.create_dm_sys(qs)
+    q.add_to_qvec_fock_op(1.0, v, qd1, 1, qd2, 1)
+    q.assemble_qvec(v)
+    assert q.get_expectation_value_qvec(v, qd1.n) == 1.0
+    assert q.get_expectation_value_qvec(v, qd2.n) == 1.0
+    assert q.get_expectation_value_qvec(v, qd1.dag, qd2) == 0.0
+    assert q.get_expectation_value_qvec(v, qd2.dag, qd1) == 0.0
+    x = v.to_numpy()
+    assert np.count_nonzero(x) == 1 and x[3 if kind == "wf" else 3 * 4 + 3] == 1.0
+    v.destroy()
+    qs.destroy()
+
+
 def test_circuit_events_inside_time_step_match_oracle(quac, oracle):
     """Gates scheduled at times inside one time_step_sys run (in-place
     engine, quantum_circuits.c:17-120): the integration stops on every

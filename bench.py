@@ -313,6 +313,50 @@ def ensemble_summary(q, n_inst=4096, tmax=100.0, dt0=0.05, plain_sample=8, tol=5
     return out
 
 
+def ensemble_sharded_summary(q, rank, world, dev, n_inst=4096, tmax=100.0, dt0=0.05, tol=5e-7):
+    """The config-4 ensemble on `world` GPUs: the instances are split over
+    the ranks longest-first by their cost (D^2 of each instance, LPT), each
+    rank integrates its share in one persistent ensemble launch (FP64
+    mode), no collective on the data path; device time between CUDA events
+    on the default stream, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from quac_b200 import systems as Sy
+    from quac_b200.replicas import lpt_partition, max_over_ranks
+    params = Sy.driven_jc_ensemble_params(n_inst)
+    costs = [(2 * p["nc"]) ** 2 for p in params]
+    shares = lpt_partition(costs, world)
+    mine = shares[rank]
+    built = []
+    for i in mine:
+        B = Sy.Builder(q)
+        Sy.driven_jc(B, **params[i])
+        built.append(B.qs)
+    E = q.Ensemble(built)
+    for qs in built:
+        qs.destroy()
+    rho0 = np.concatenate([Sy.excited_vacuum(params[i]["nc"]) for i in mine])
+    E.set_options(precision=0, atol=tol, rtol=tol)
+    E.set_states(rho0)
+    E.run(0.0, 0.5, dt0)  # captures the graph
+    E.set_states(rho0)
+    torch.cuda.synchronize()
+    dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(torch.cuda.default_stream(dev))
+    E.run(0.0, tmax, dt0)
+    ev1.record(torch.cuda.default_stream(dev))
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    loads = [sum(costs[i] for i in s) for s in shares]
+    [ms_max] = max_over_ranks([ms], device=dev)
+    E.destroy()
+    return {"workload": f"driven_jc_ensemble_{n_inst}", "t_end": tmax, "controller": f"DP5(4) atol=rtol={tol:g}",
+            "partition": "longest-first by D^2 over ranks (lpt_partition)", "instances_per_rank":
+            [len(s) for s in shares], "cost_imbalance": max(loads) / (sum(loads) / world),
+            "solves_per_s": n_inst / (ms_max / 1e3), "ms_max_over_ranks": ms_max}
+
+
 def precision_summary(q, qs, rho, x0, stream, steps, segment):
     """12-qubit TFIM with complex64 contraction: the headline segment timed
     again, and the full run of that workload (Dormand-Prince 5(4),
@@ -586,6 +630,9 @@ def run_ours(args, rank, world, local_rank):
                       "note": "Hermitian mode off: both passes compute and store every element (segments after "
                               "the timed region, same workload)"},
     }
+    if world > 1 and not args.no_ensemble:
+        # every rank takes part (its share of the instances, one max over ranks)
+        out["ensemble_sharded"] = ensemble_sharded_summary(q, rank, world, dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0 and world == 1 and not args.no_ensemble:

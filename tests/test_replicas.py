@@ -56,3 +56,18 @@ def test_max_over_ranks_gloo_world2():
     res.sort()
     assert res[0][1] == [20.0, 0.0] and res[1][1] == [20.0, 0.0]
     assert sorted(res[0][2] + res[1][2]) == [0, 1, 2, 3, 4]
+
+
+def test_config4_ensemble_shards():
+    """The sharded ensemble of bench.py --gpus N: the 4096 driven-JC
+    instances split over 2, 4 and 8 ranks, each instance once, the D^2
+    loads within one instance of each other."""
+    from quac_b200 import systems as Sy
+    params = Sy.driven_jc_ensemble_params(4096)
+    costs = np.array([(2 * p["nc"]) ** 2 for p in params])
+    for world in (2, 4, 8):
+        parts = lpt_partition(costs, world)
+        assert sorted(i for p in parts for i in p) == list(range(4096))
+        loads = [costs[np.array(p)].sum() for p in parts]
+        assert max(loads) - min(loads) <= costs.max()
+        assert all(costs[p[k]] >= costs[p[k + 1]] for p in parts for k in range(len(p) - 1))

@@ -209,6 +209,11 @@ void create_dm_sys(qsystem qsys, qvec *q);              /* qvec_utilities.c:650-
 void create_wf_sys(qsystem qsys, qvec *q);              /* qvec_utilities.c:705-763 */
 void create_arb_qvec(qvec *q, PetscInt nstates, qvec_type type);      /* qvec_utilities.c:471-521 */
 void destroy_qvec(qvec *q);                             /* qvec_utilities.c:1076-1091 */
+/* The variadic locations of add_to_qvec (row, col for a density matrix, the
+ * index for a wavefunction) are read as PetscInt (int64_t), as in the
+ * reference; the Fock states of add_to_qvec_fock_op / get_qvec_loc_fock_op
+ * are read from the low 32 bits of their argument slots, so int literals
+ * and PetscInt values both work there (a state is below its op's levels). */
 void add_to_qvec(qvec q, PetscScalar alpha, ...);       /* qvec_utilities.c:919-969 */
 void add_to_qvec_loc(qvec q, PetscScalar alpha, PetscInt loc);        /* qvec_utilities.c:879-897 */
 /* Basis states by Fock occupations: (op, PetscInt fock state) pairs; the

@@ -684,7 +684,7 @@ void get_qvec_loc_fock_op(qvec q, PetscInt *loc, PetscInt num_ops, ...) {
   va_start(ap, num_ops);
   for (size_t i = 0; i < ops.size(); i++) {
     ops[i] = va_arg(ap, op_handle);
-    fock[i] = va_arg(ap, PetscInt);
+    fock[i] = (PetscInt)(int32_t)va_arg(ap, PetscInt);  // an int or a PetscInt argument
   }
   va_end(ap);
   get_qvec_loc_fock_op_list(q, loc, num_ops, ops.data(), fock.data());
@@ -704,7 +704,7 @@ void add_to_qvec_fock_op(PetscScalar alpha, qvec q, PetscInt num_ops, ...) {
   va_start(ap, num_ops);
   for (size_t i = 0; i < ops.size(); i++) {
     ops[i] = va_arg(ap, op_handle);
-    fock[i] = va_arg(ap, PetscInt);
+    fock[i] = (PetscInt)(int32_t)va_arg(ap, PetscInt);  // an int or a PetscInt argument
   }
   va_end(ap);
   add_to_qvec_fock_op_list(alpha, q, num_ops, ops.data(), fock.data());

@@ -82,3 +82,21 @@ def test_c_ensemble_program_matches_oracle(quac, oracle, tmp_path):
         oracle.free_csr(h)
         rho = y.reshape(D, D, order="F")
         assert abs(pe - rho.diagonal().real[nc:].sum()) < 1e-10, i
+
+
+def test_c_fock_loc_with_int_literals(quac, tmp_path):
+    """get_qvec_loc_fock_op called from C with int literals for the Fock
+    states (four pairs, so some travel on the stack): the index is
+    sum fock_i * n_before_i = 1 + 2*2 + 3*6 + 1*24 = 47 (qvec_utilities.c:
+    996-1033), and 47 * 48 + 47 for a density matrix."""
+    exe = tmp_path / "fock_loc"
+    libdir = os.path.join(ROOT, "quac_b200")
+    cmd = ["/usr/bin/gcc", "-std=c99", "-O2", "-Wall", "-I", os.path.join(ROOT, "include", "quac"),
+           os.path.join(ROOT, "tests", "c", "fock_loc.c"), "-o", str(exe), "-L", libdir,
+           "-lquac_b200", f"-Wl,-rpath,{libdir}", "-lm"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = dict(ln.split() for ln in r.stdout.splitlines())
+    assert got == {"wf": "47", "dm": str(47 * 48 + 47)}

@@ -398,11 +398,35 @@ def precision_summary(q, qs, rho, x0, stream, steps, segment):
     q.set_ts_options(rk_type="4", adapt_type="none", rtol=5e-7, atol=5e-7)
     a, b = states
     out["run_t50_seconds"] = {"fp64": secs[0], "fp32_contraction": secs[1]}
+    # Uhlmann fidelity (Tr sqrt(sqrt(a) b sqrt(a)))^2 of the two final
+    # states, eigen-decompositions by torch on the GPU (measurement only)
+    ta = torch.from_numpy((a + a.conj().T) / 2).cuda()
+    tb = torch.from_numpy((b + b.conj().T) / 2).cuda()
+    w, V = torch.linalg.eigh(ta)
+    sa = (V * torch.sqrt(torch.clamp(w, min=0.0))) @ V.conj().T
+
+    def uhlmann(t):
+        ev = torch.linalg.eigvalsh(sa @ t @ sa)
+        return float(torch.sum(torch.sqrt(torch.clamp(ev, min=0.0))) ** 2)
+
+    fid = uhlmann(tb)
+    # the same computation of the complex128 state against itself: the floor
+    # set by the eigen-decompositions (sqrt of the state's rounding-level
+    # eigenvalues), not by the complex64 contraction
+    fid_self = uhlmann(ta)
+    neg = float(-torch.clamp(w, max=0.0).sum())
+    del ta, tb, w, V, sa
     out["errors_vs_fp64"] = {
         "trace": float(abs(np.trace(b) - np.trace(a))),
         "population_max": float(np.abs(a.diagonal().real - b.diagonal().real).max()),
         "state_rel_frobenius": float(np.linalg.norm(a - b) / np.linalg.norm(a)),
         "purity": float(abs(np.vdot(b, b).real - np.vdot(a, a).real)),
+        # F(fp64, complex64) against F(fp64, fp64): the adaptive run's state
+        # has slightly negative eigenvalues, which puts F(fp64, fp64) itself
+        # below 1 by about twice their sum
+        "fidelity": abs(fid - fid_self),
+        "fidelity_floor_fp64_vs_itself": abs(1.0 - fid_self),
+        "fp64_state_negative_eigenvalue_sum": neg,
     }
     return out
 

@@ -157,6 +157,8 @@ __device__ __forceinline__ void tma_tile(const PassParams &P, const CUtensorMap 
   tile_origin(P, t, rfix, cfix);
   const unsigned long long F = (unsigned long long)rfix | ((unsigned long long)cfix << P.n);
   int c[5] = {0, 0, 0, 0, 0};
+  // a fixed run merged into dim 0: two doubles per element
+  if (!P.tfree[0]) c[0] = (int)(2ull * (F & ((1ull << P.tlen[0]) - 1ull)));
 #pragma unroll
   for (int d = 1; d < 5; d++)
     c[d] = P.tfree[d] ? 0 : (int)((F >> P.tstart[d]) & ((1ull << P.tlen[d]) - 1ull));
@@ -218,7 +220,11 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
   // last pass with TMA: the first stage base of each tile comes by TMA into
   // the third buffer, and the tiles of x use two stages
   const bool bt = TMA && P.last && E.nupd > 0 && E.base[0] != nullptr;
-  const int nst = TMA ? (bt ? 2 : 3) : 2;
+  // a middle pass (running sum in and out, complex128): its running-sum tile
+  // comes by TMA into the third buffer (the tensor map in bmap) and is added
+  // after the pass's own terms, instead of single 16-byte loads per thread
+  const bool at = TMA && !F32 && !P.last && P.accin != nullptr;
+  const int nst = TMA ? ((bt || at) ? 2 : 3) : 2;
   const double2 *bbuf = sm + 2 * NEL;
   const int n = P.n, lo = P.lo;
   const size_t D = (size_t)1 << n;
@@ -256,7 +262,7 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
       const long long t2 = (long long)atomicAdd(P.claim, 1ull);
       tids[q2] = t2;
       if (t2 < P.ntiles) tma_tile(P, &tmap, sm + q2 * NEL, &bars[q2], t2);
-      if (bt) tma_tile(P, &bmap, sm + 2 * NEL, &bars[3], t);
+      if (bt || at) tma_tile(P, &bmap, sm + 2 * NEL, &bars[3], t);
     }
     unsigned rfix, cfix;
     tile_origin(P, t, rfix, cfix);
@@ -273,7 +279,7 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
     for (int m = 0; m < QMC; m++) c[m] = cfix | (cl[m] << lo);
     // loads that do not depend on the tile go out before the wait
     V2 acc[2][QMC];
-    if (P.accin) {
+    if (P.accin && !at) {
       const V2 *ain = reinterpret_cast<const V2 *>(P.accin);
 #pragma unroll
       for (int i = 0; i < 2; i++)
@@ -505,9 +511,19 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
         }
       }
     }
-    if (bt) {
+    if (bt || at) {
       const bool ok = mbar_wait_bounded(&bars[3], (unsigned)(it & 1), 2000000000ull);
       if (__syncthreads_or(!ok)) { timed_out = true; break; }
+    }
+    if (at) {
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int m = 0; m < QMC; m++) {
+          const double2 v = bbuf[cl[m] * 64 + rl[i]];
+          acc[i][m].x += v.x;
+          acc[i][m].y += v.y;
+        }
     }
     // first stage base of element (i, m)
     auto base0 = [&](int i, int m, size_t idx) -> double2 {
@@ -613,7 +629,7 @@ __global__ void __launch_bounds__(QT, 1) k_qpass(const __grid_constant__ PassPar
         const int q = (it + k2) % nst;
         if (tids[q] < P.ntiles) mbar_wait_bounded(&bars[q], (unsigned)(((it + k2) / nst) & 1), 500000000ull);
       }
-      if (bt) mbar_wait_bounded(&bars[3], (unsigned)(it & 1), 500000000ull);
+      if (bt || at) mbar_wait_bounded(&bars[3], (unsigned)(it & 1), 500000000ull);
     }
     // queue reset by the last CTA: every CTA has made its final claim
     // before it counts itself here
@@ -682,14 +698,27 @@ bool describe_tma(PassParams &pp) {
   add(n, lo, false);
   add(n + lo, 6, true);
   add(n + lo + 6, n - lo - 6, false);
-  // dim 0 = the element (two doubles), merged with a leading free run
+  // dim 0 = the element (two doubles), merged with a leading free run; when
+  // the runs need more than five dimensions (a middle group: fixed bits on
+  // both sides of the free ones in rows and columns), a leading fixed run
+  // is merged into dim 0 as well, its value selected by the dim-0
+  // coordinate (an even number of doubles, so 16-byte aligned) with a box
+  // of one element
   int first = 0;
-  if (!runs.empty() && runs[0].start == 0 && runs[0].free) first = 1;
+  bool first_fixed = false;
+  if (!runs.empty() && runs[0].start == 0) {
+    if (runs[0].free) {
+      first = 1;
+    } else if (1 + (int)runs.size() > 5) {
+      first = 1;
+      first_fixed = true;
+    }
+  }
   const int ndims = 1 + (int)runs.size() - first;
   if (ndims > 5) return false;
   pp.tstart[0] = 0;
   pp.tlen[0] = first ? runs[0].len : 0;
-  pp.tfree[0] = 1;
+  pp.tfree[0] = first_fixed ? 0 : 1;
   int d = 1;
   for (size_t k = first; k < runs.size(); k++, d++) {
     pp.tstart[d] = runs[k].start;
@@ -708,7 +737,7 @@ void encode_tma(const PassParams &pp, const double2 *x, CUtensorMap *map) {
   cuuint64_t dims[5], strides[4];
   cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
   dims[0] = 2ull << pp.tlen[0];
-  box[0] = 2u << pp.tlen[0];
+  box[0] = pp.tfree[0] ? (2u << pp.tlen[0]) : 2u;
   for (int d = 1; d < 5; d++) {
     dims[d] = 1ull << pp.tlen[d];
     box[d] = pp.tfree[d] ? (1u << pp.tlen[d]) : 1u;
@@ -967,6 +996,8 @@ void launch_qubit_passes(std::vector<PassParams> &passes, const double2 *x, doub
     if (pp.tma) encode_tma(pp, x, &map);
     // the kernel loads the first stage base by TMA in a last pass with TMA
     if (pp.tma && pp.last && e.nupd > 0 && e.base[0]) encode_tma(pp, e.base[0], &bmap);
+    // a middle pass with TMA reads its running sum through bmap (complex128)
+    if (pp.tma && !pp.last && pp.accin && !f32) encode_tma(pp, pp.accin, &bmap);
     const int g = (int)std::min<long long>(pp.ntiles, num_sms());
     if (f32) launch_any_pass<true>(pp, map, bmap, x, e, g, pass_smem(pp), s, false);
     else launch_any_pass<false>(pp, map, bmap, x, e, g, pass_smem(pp), s, false);

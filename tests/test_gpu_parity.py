@@ -682,3 +682,26 @@ def test_hermitian_mode_lx_d4096_matches_oracle_rows(quac, oracle):
     yfull = quac.lrho_apply_host(S.qs, x)
     assert _rel(y, yfull) < 1e-13
     S.qs.destroy()
+
+
+@pytest.mark.parametrize("build", [tfim_real, tfim_pump], ids=["tfim13", "pump13"])
+def test_three_pass_lx_d8192_matches_oracle_rows(quac, oracle, build):
+    """13 qubits: three passes, the middle one over bits 6-11 with fixed bits
+    on both sides of its free ones (its TMA box takes the low fixed bits
+    into the element dimension, selected by the innermost coordinate).
+    L.x of a random (non-Hermitian) vector against the oracle's rows for a
+    low and a high column range."""
+    S = H.ProductSystem(quac)
+    O = oracle.OSys()
+    build(S, 13)
+    build(O, 13)
+    quac.construct_matrix(S.qs)
+    D = S.D
+    rng = np.random.default_rng(25)
+    x = rng.normal(size=D * D) + 1j * rng.normal(size=D * D)
+    y = quac.lrho_apply_host(S.qs, x)
+    for c_lo, c_hi in [(3, 5), (8189, 8192)]:
+        r0, r1 = c_lo * D, c_hi * D
+        Ablk = O.liouvillian(rows=(r0, r1))
+        assert _rel(y[r0:r1], Ablk @ x) < 1e-12
+    S.qs.destroy()
